@@ -1,0 +1,77 @@
+// pt_device.h — device memory ownership and launch helpers (CUDA runtime, host side).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <string>
+#include <vector>
+#include "pt_host.h"
+
+namespace ptb {
+
+inline void cuda_check(cudaError_t result, const char *what) {
+    if(result != cudaSuccess) throw Error(PT_CUDA_ERROR, std::string(what) + ": " + cudaGetErrorString(result));
+}
+#define PT_CUDA(call) ::ptb::cuda_check((call), #call)
+
+// Owning device allocation (the library's only allocator).
+class DeviceBuffer {
+public:
+    DeviceBuffer() = default;
+    explicit DeviceBuffer(size_t bytes) { resize(bytes); }
+    ~DeviceBuffer() { release(); }
+    DeviceBuffer(const DeviceBuffer &) = delete;
+    DeviceBuffer &operator=(const DeviceBuffer &) = delete;
+    DeviceBuffer(DeviceBuffer &&o) noexcept : ptr_(o.ptr_), bytes_(o.bytes_) { o.ptr_ = nullptr; o.bytes_ = 0; }
+    void resize(size_t bytes) {
+        if(bytes == bytes_) return;
+        release();
+        if(bytes) PT_CUDA(cudaMalloc(&ptr_, bytes));
+        bytes_ = bytes;
+    }
+    void reserve(size_t bytes) { if(bytes > bytes_) resize(bytes); }
+    template <class T> void upload(const std::vector<T> &v) {
+        resize(v.size() * sizeof(T));
+        if(bytes_) PT_CUDA(cudaMemcpy(ptr_, v.data(), bytes_, cudaMemcpyHostToDevice));
+    }
+    void upload(const void *src, size_t bytes) {
+        resize(bytes);
+        if(bytes) PT_CUDA(cudaMemcpy(ptr_, src, bytes, cudaMemcpyHostToDevice));
+    }
+    template <class T = void> T *get() const { return static_cast<T *>(ptr_); }
+    size_t bytes() const { return bytes_; }
+    void release() { if(ptr_) cudaFree(ptr_); ptr_ = nullptr; bytes_ = 0; }
+private:
+    void *ptr_ = nullptr;
+    size_t bytes_ = 0;
+};
+
+class Event {
+public:
+    Event() { PT_CUDA(cudaEventCreate(&e_)); }
+    ~Event() { cudaEventDestroy(e_); }
+    Event(const Event &) = delete;
+    Event &operator=(const Event &) = delete;
+    cudaEvent_t get() const { return e_; }
+private:
+    cudaEvent_t e_{};
+};
+
+void require_device();
+int device_sm_count();
+
+} // namespace ptb
+
+// The scene handle: everything device-resident that queries and renderers read.
+struct pt_scene {
+    ptb::DeviceScene view{};
+    ptb::DeviceBuffer nodes, tris, spheres, triangles, sphere_src, materials, textures, pixels, lights, brute_order;
+    std::vector<pt_light> host_lights;
+    float light_area = 0;
+    int32_t leaf_count = 0;
+    size_t triangle_count = 0, sphere_count = 0;
+    // host-buffer query workspace (reused between calls)
+    ptb::DeviceBuffer work_rays[3], work_tmax[3], work_hits[3], work_stats[3];
+    cudaStream_t streams[3] = {nullptr, nullptr, nullptr};
+    int device = 0;
+    ~pt_scene();
+};

@@ -1,0 +1,75 @@
+// pt_internal.h — device-side layouts of the B200 path-tracing core (shared host/device).
+//
+// HBM layout of a scene (all arrays 16-byte aligned, read with 16-byte vector loads):
+//   nodes    : one 64-byte record per branch of the caller's flattened BVH, holding the
+//              boxes of BOTH children (two-child "boxes in the parent" layout), so one
+//              node fetch answers two box tests.
+//   tris     : one 48-byte record per triangle leaf, {v0, eps}, {e1, id}, {e2, -}, where
+//              e1 = v1-v0, e2 = v2-v0 and eps = 1e-7f*|e1 x e2| are computed on the host
+//              with the same FP32 operations the reference performs per test
+//              (src/flat/flat_intersect.h:10-18), so the device test is bit-identical.
+//   spheres  : one 32-byte record per sphere leaf {center, radius}, {id, -, -, -}.
+//   shading  : the caller's flat_triangle / flat_sphere / flat_material / flat_texture
+//              arrays, untouched, read only for the winning hit of a ray.
+#pragma once
+
+#include <cstdint>
+#include "../../include/pt.h"
+
+#ifdef __CUDACC__
+#define PT_HD __host__ __device__
+#else
+#define PT_HD
+#endif
+
+namespace ptb {
+
+// Child reference: >= 0 internal node; < 0 leaf slot ~child.  Slots [0, tri_slots) are
+// triangles, [tri_slots, tri_slots + sphere_slots) spheres.
+constexpr int32_t kEmptyChild = 0x7fffffff;
+constexpr int kStackCapacity = 64;   // flat_stack_capacity, src/flat/flat_data.h:52
+
+struct alignas(16) BvhNode {
+    // child 0 box x/y, child 1 box x/y, both boxes' z, children
+    float c0lox, c0hix, c0loy, c0hiy;
+    float c1lox, c1hix, c1loy, c1hiy;
+    float c0loz, c0hiz, c1loz, c1hiz;
+    int32_t child0, child1, pad0, pad1;
+};
+static_assert(sizeof(BvhNode) == 64, "node is 64 bytes");
+
+struct alignas(16) TriRecord {
+    float v0x, v0y, v0z, eps;
+    float e1x, e1y, e1z; int32_t id;
+    float e2x, e2y, e2z; int32_t node;   // flat node index of the leaf (reference tie order)
+};
+static_assert(sizeof(TriRecord) == 48, "triangle record is 48 bytes");
+
+struct alignas(16) SphereRecord {
+    float cx, cy, cz, radius;
+    int32_t id, node, pad0, pad1;
+};
+static_assert(sizeof(SphereRecord) == 32, "sphere record is 32 bytes");
+
+// Everything a kernel needs, passed by value (device pointers).
+struct DeviceScene {
+    const BvhNode *nodes;
+    const TriRecord *tris;
+    const SphereRecord *spheres;
+    const pt_triangle *triangles;   // caller's records (shading, light sampling)
+    const pt_sphere *sphere_src;
+    const pt_material *materials;
+    const pt_texture *textures;
+    const unsigned char *pixels;
+    const pt_light *lights;
+    int32_t node_count;             // internal nodes (0 for an empty scene)
+    int32_t tri_slots, sphere_slots;
+    int32_t light_count;
+    float light_area;
+    int32_t empty;                  // root == -1
+};
+
+// Tie rule for exact-distance hits.
+enum TieRule : int { kTieLowestId = 0, kTieLastLeaf = 1 };
+
+} // namespace ptb

@@ -1,0 +1,359 @@
+// pt_query.cu — scene upload and the ray-query kernels (sm_100a, built with --fmad=false).
+//
+// Replaces cuda_query_rays / query_rays (src/cuda/cuda_renderer.cu:111-120, 248-260) and the
+// device_scene upload (src/cuda/cuda_renderer.cu:36-54).
+#include <cfloat>
+#include <cstring>
+#include <mutex>
+#include "pt_api_common.h"
+#include "pt_device.h"
+#include "pt_traverse.h"
+
+using namespace ptb;
+
+namespace ptb {
+
+static thread_local std::string g_last_error;
+void set_last_error(const std::string &message) { g_last_error = message; }
+
+void require_device() {
+    int count = 0;
+    cudaError_t st = cudaGetDeviceCount(&count);
+    if(st != cudaSuccess) { cudaGetLastError(); throw Error(PT_NO_DEVICE, std::string("CUDA device unavailable: ") + cudaGetErrorString(st)); }
+    if(count < 1) throw Error(PT_NO_DEVICE, "CUDA device unavailable: no CUDA devices");
+}
+
+int device_sm_count() {
+    int dev = 0, sms = 0;
+    PT_CUDA(cudaGetDevice(&dev));
+    PT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    return sms;
+}
+
+constexpr int kQueryBlock = 128;
+
+template <bool kAny, bool kStats>
+__global__ void __launch_bounds__(kQueryBlock) query_kernel(DeviceScene s, const pt_ray *__restrict__ rays, size_t count,
+                                                            float tmin, const float *__restrict__ tmax,
+                                                            pt_hit *__restrict__ hits, pt_ray_stats *__restrict__ stats, int tie) {
+    size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if(i >= count) return;
+    pt_ray r = rays[i];
+    float hi = tmax ? tmax[i] : FLT_MAX;
+    HitInfo h;
+    uint32_t boxes = 0, prims = 0;
+    int error = 0;
+    bool hit = traverse<kAny>(s, r, tmin, hi, tie, h, boxes, prims, error);
+    int32_t type = PT_BRANCH, id = -1;
+    if(hit) hit_ids(s, h.slot, type, id);
+    int4 out = make_int4(__float_as_int(hit ? h.t : 0.0f), id, type, error);
+    reinterpret_cast<int4 *>(hits)[i] = out;
+    if(kStats) { stats[i].boxes = boxes; stats[i].primitives = prims; }
+}
+
+template <bool kAny, bool kStats>
+__global__ void __launch_bounds__(kQueryBlock) brute_kernel(DeviceScene s, const int32_t *__restrict__ order, int32_t leaves,
+                                                            const pt_ray *__restrict__ rays, size_t count, float tmin,
+                                                            const float *__restrict__ tmax, pt_hit *__restrict__ hits,
+                                                            pt_ray_stats *__restrict__ stats, int tie) {
+    size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if(i >= count) return;
+    pt_ray r = rays[i];
+    float hi = tmax ? tmax[i] : FLT_MAX;
+    HitInfo h;
+    uint32_t prims = 0;
+    bool hit = traverse_brute<kAny>(s, order, leaves, r, tmin, hi, tie, h, prims);
+    int32_t type = PT_BRANCH, id = -1;
+    if(hit) hit_ids(s, h.slot, type, id);
+    reinterpret_cast<int4 *>(hits)[i] = make_int4(__float_as_int(hit ? h.t : 0.0f), id, type, 0);
+    if(kStats) { stats[i].boxes = 0; stats[i].primitives = prims; }
+}
+
+// query_rays (src/cuda/cuda_renderer.cu:111-120): full trace_result, reference tie rule.
+__global__ void __launch_bounds__(kQueryBlock) compat_kernel(DeviceScene s, const int32_t *__restrict__ order, int32_t leaves,
+                                                             const pt_ray *__restrict__ rays, size_t count, int brute,
+                                                             pt_trace_result *__restrict__ out) {
+    size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if(i >= count) return;
+    pt_ray r = rays[i];
+    HitInfo h;
+    uint32_t boxes = 0, prims = 0;
+    int error = 0;
+    bool hit = brute ? traverse_brute<false>(s, order, leaves, r, 0.001f, FLT_MAX, kTieLastLeaf, h, prims)
+                     : traverse<false>(s, r, 0.001f, FLT_MAX, kTieLastLeaf, h, boxes, prims, error);
+    pt_trace_result res;
+    res.rec.t = 0; res.rec.u = 0; res.rec.v = 0;
+    res.rec.p = pt_vec3{0, 0, 0}; res.rec.normal = pt_vec3{0, 0, 0};
+    res.rec.material_id = -1; res.rec.primitive_type = -1; res.rec.primitive_id = -1;
+    if(hit) finalize_hit(s, r, h, res.rec);
+    res.hit = hit ? 1 : 0;
+    res.error = error;
+    out[i] = res;
+}
+
+// Camera rays, one PCG stream per ray (same arithmetic as pt_rays_camera on the host).
+__global__ void camera_rays_kernel(pt_camera c, int width, int height, uint64_t seed, uint64_t first, size_t count, pt_ray *rays) {
+    size_t k = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if(k >= count) return;
+    uint64_t index = first + k;
+    uint64_t pixel = index % (uint64_t(width) * uint64_t(height));
+    int x = int(pixel % uint64_t(width)), y = int(pixel / uint64_t(width));
+    Pcg r; r.seed(seed, index);
+    float u = (x + r.uniform()) / float(width);
+    float v = (y + r.uniform()) / float(height);
+    pt_ray out;
+    camera_ray(c, u, v, r, out);
+    rays[k] = out;
+}
+
+// Bounce rays: from each primary hit, a cosine-distributed direction about the geometric
+// normal turned toward the incoming ray; a primary miss is replaced by a random surface ray.
+__global__ void bounce_rays_kernel(DeviceScene s, const pt_ray *primary, const pt_hit *hits, size_t count,
+                                   uint64_t seed, uint64_t first, uint64_t triangles, pt_ray *out) {
+    size_t k = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if(k >= count) return;
+    pt_ray r = primary[k];
+    pt_hit h = hits[k];
+    Pcg g; g.seed(seed, first + k);
+    f3 p, n;
+    f3 d = mk(r.direction);
+    if(h.primitive_type == PT_TRIANGLE) {
+        const pt_triangle &t = s.triangles[h.primitive_id];
+        p = mk(r.origin) + h.t * d;
+        n = unit(cross(mk(t.v1) - mk(t.v0), mk(t.v2) - mk(t.v0)));
+        if(dot(n, d) > 0) n = -n;
+    } else if(h.primitive_type == PT_SPHERE) {
+        const pt_sphere &sp = s.sphere_src[h.primitive_id];
+        p = mk(r.origin) + h.t * d;
+        n = (p - mk(sp.center)) / sp.radius;
+        if(dot(n, d) > 0) n = -n;
+    } else {
+        surface_point(s.triangles, triangles, g, p, n);
+    }
+    pt_ray o;
+    o.origin = pv(p);
+    o.direction = pv(cosine_lift(n, g));
+    o.time = r.time;
+    out[k] = o;
+}
+
+unsigned grid_for(size_t count, int block) { return unsigned((count + size_t(block) - 1) / size_t(block)); }
+
+void launch_query(const pt_scene *sc, const pt_ray *rays, size_t count, int mode, float tmin, const float *tmax,
+                  pt_hit *hits, pt_ray_stats *stats, int tie, cudaStream_t stream) {
+    if(!count) return;
+    unsigned grid = grid_for(count, kQueryBlock);
+    const DeviceScene &s = sc->view;
+    if(mode == PT_QUERY_ANY) {
+        if(stats) query_kernel<true, true><<<grid, kQueryBlock, 0, stream>>>(s, rays, count, tmin, tmax, hits, stats, tie);
+        else query_kernel<true, false><<<grid, kQueryBlock, 0, stream>>>(s, rays, count, tmin, tmax, hits, stats, tie);
+    } else {
+        if(stats) query_kernel<false, true><<<grid, kQueryBlock, 0, stream>>>(s, rays, count, tmin, tmax, hits, stats, tie);
+        else query_kernel<false, false><<<grid, kQueryBlock, 0, stream>>>(s, rays, count, tmin, tmax, hits, stats, tie);
+    }
+    PT_CUDA(cudaGetLastError());
+}
+
+} // namespace ptb
+
+pt_scene::~pt_scene() {
+    for(auto &s : streams) if(s) cudaStreamDestroy(s);
+}
+
+extern "C" {
+
+const char *pt_last_error(void) { return g_last_error.c_str(); }
+int pt_abi_version(void) { return PT_ABI_VERSION; }
+
+// cuda_device_available, src/cuda/cuda_renderer.cu:128-140
+int pt_device_available(char *description, size_t capacity) {
+    std::string text;
+    int ok = 0;
+    int count = 0;
+    cudaError_t status = cudaGetDeviceCount(&count);
+    if(status != cudaSuccess) { text = cudaGetErrorString(status); cudaGetLastError(); }
+    else if(count < 1) text = "no CUDA devices";
+    else {
+        int current = 0;
+        cudaDeviceProp properties{};
+        status = cudaGetDevice(&current);
+        if(status == cudaSuccess) status = cudaGetDeviceProperties(&properties, current);
+        if(status != cudaSuccess) text = cudaGetErrorString(status);
+        else { text = properties.name; ok = 1; }
+    }
+    if(description && capacity) {
+        std::strncpy(description, text.c_str(), capacity - 1);
+        description[capacity - 1] = 0;
+    }
+    return ok;
+}
+
+pt_status pt_scene_create(const pt_scene_desc *desc, pt_scene **out) {
+    return guard([&]() {
+        if(!desc || !out) throw Error(PT_INVALID_ARGUMENT, "null argument");
+        *out = nullptr;
+        validate_scene(*desc);
+        require_device();
+        float area = 0;
+        std::vector<pt_light> lights = scene_lights(*desc, area);
+        HostLayout layout = relayout(*desc);
+        auto sc = new pt_scene;
+        try {
+            PT_CUDA(cudaGetDevice(&sc->device));
+            sc->host_lights = lights;
+            sc->light_area = area;
+            sc->triangle_count = desc->triangle_count;
+            sc->sphere_count = desc->sphere_count;
+            sc->nodes.upload(layout.nodes);
+            sc->tris.upload(layout.tris);
+            sc->spheres.upload(layout.spheres);
+            sc->brute_order.upload(layout.brute_order);
+            sc->triangles.upload(desc->triangles, desc->triangle_count * sizeof(pt_triangle));
+            sc->sphere_src.upload(desc->spheres, desc->sphere_count * sizeof(pt_sphere));
+            sc->materials.upload(desc->materials, desc->material_count * sizeof(pt_material));
+            sc->textures.upload(desc->textures, desc->texture_count * sizeof(pt_texture));
+            sc->pixels.upload(desc->pixels, desc->pixel_bytes);
+            sc->lights.upload(lights);
+            sc->leaf_count = int32_t(layout.brute_order.size());
+            DeviceScene &v = sc->view;
+            v.nodes = sc->nodes.get<BvhNode>();
+            v.tris = sc->tris.get<TriRecord>();
+            v.spheres = sc->spheres.get<SphereRecord>();
+            v.triangles = sc->triangles.get<pt_triangle>();
+            v.sphere_src = sc->sphere_src.get<pt_sphere>();
+            v.materials = sc->materials.get<pt_material>();
+            v.textures = sc->textures.get<pt_texture>();
+            v.pixels = sc->pixels.get<unsigned char>();
+            v.lights = sc->lights.get<pt_light>();
+            v.node_count = int32_t(layout.nodes.size());
+            v.tri_slots = int32_t(layout.tris.size());
+            v.sphere_slots = int32_t(layout.spheres.size());
+            v.light_count = int32_t(lights.size());
+            v.light_area = area;
+            v.empty = layout.empty;
+        } catch(...) { delete sc; throw; }
+        *out = sc;
+    });
+}
+
+pt_status pt_scene_destroy(pt_scene *scene) { delete scene; return PT_OK; }
+
+pt_status pt_scene_lights(const pt_scene *scene, pt_light *lights, size_t capacity, size_t *count, float *total_area) {
+    return guard([&]() {
+        if(!scene) throw Error(PT_INVALID_ARGUMENT, "null scene");
+        if(count) *count = scene->host_lights.size();
+        if(total_area) *total_area = scene->light_area;
+        for(size_t i = 0; i < capacity && i < scene->host_lights.size(); i++) lights[i] = scene->host_lights[i];
+    });
+}
+
+pt_status pt_scene_device_bytes(const pt_scene *s, size_t *bytes) {
+    return guard([&]() {
+        if(!s || !bytes) throw Error(PT_INVALID_ARGUMENT, "null argument");
+        *bytes = s->nodes.bytes() + s->tris.bytes() + s->spheres.bytes() + s->triangles.bytes() + s->sphere_src.bytes() +
+                 s->materials.bytes() + s->textures.bytes() + s->pixels.bytes() + s->lights.bytes() + s->brute_order.bytes();
+    });
+}
+
+pt_status pt_query_rays_device(const pt_scene *scene, const pt_ray *rays, size_t count, int mode, float tmin,
+                               const float *tmax, pt_hit *hits, pt_ray_stats *stats, void *stream) {
+    return guard([&]() {
+        if(!scene || (count && (!rays || !hits))) throw Error(PT_INVALID_ARGUMENT, "null argument");
+        if(mode != PT_QUERY_CLOSEST && mode != PT_QUERY_ANY) throw Error(PT_INVALID_ARGUMENT, "unknown query mode");
+        launch_query(scene, rays, count, mode, tmin, tmax, hits, stats, kTieLowestId, static_cast<cudaStream_t>(stream));
+    });
+}
+
+// Brute-force form (every leaf, node-array order); used for parity checks.
+pt_status pt_query_rays_brute_device(const pt_scene *scene, const pt_ray *rays, size_t count, int mode, float tmin,
+                                     const float *tmax, pt_hit *hits, pt_ray_stats *stats, void *stream) {
+    return guard([&]() {
+        if(!scene || (count && (!rays || !hits))) throw Error(PT_INVALID_ARGUMENT, "null argument");
+        if(!count) return;
+        unsigned grid = grid_for(count, kQueryBlock);
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        const int32_t *order = scene->brute_order.get<int32_t>();
+        if(mode == PT_QUERY_ANY) {
+            if(stats) brute_kernel<true, true><<<grid, kQueryBlock, 0, st>>>(scene->view, order, scene->leaf_count, rays, count, tmin, tmax, hits, stats, kTieLowestId);
+            else brute_kernel<true, false><<<grid, kQueryBlock, 0, st>>>(scene->view, order, scene->leaf_count, rays, count, tmin, tmax, hits, stats, kTieLowestId);
+        } else {
+            if(stats) brute_kernel<false, true><<<grid, kQueryBlock, 0, st>>>(scene->view, order, scene->leaf_count, rays, count, tmin, tmax, hits, stats, kTieLowestId);
+            else brute_kernel<false, false><<<grid, kQueryBlock, 0, st>>>(scene->view, order, scene->leaf_count, rays, count, tmin, tmax, hits, stats, kTieLowestId);
+        }
+        PT_CUDA(cudaGetLastError());
+    });
+}
+
+// Host buffers: chunks of rays flow through three streams so the upload of one chunk, the
+// traversal of the next and the download of a third overlap.
+pt_status pt_query_rays(const pt_scene *cscene, const pt_ray *rays, size_t count, int mode, float tmin,
+                        const float *tmax, pt_hit *hits, pt_ray_stats *stats) {
+    return guard([&]() {
+        pt_scene *scene = const_cast<pt_scene *>(cscene);
+        if(!scene || (count && (!rays || !hits))) throw Error(PT_INVALID_ARGUMENT, "null argument");
+        if(mode != PT_QUERY_CLOSEST && mode != PT_QUERY_ANY) throw Error(PT_INVALID_ARGUMENT, "unknown query mode");
+        if(!count) return;
+        const size_t chunk = size_t(1) << 22;
+        size_t per = count < chunk ? count : chunk;
+        for(int k = 0; k < 3; k++) {
+            if(!scene->streams[k]) PT_CUDA(cudaStreamCreateWithFlags(&scene->streams[k], cudaStreamNonBlocking));
+            scene->work_rays[k].reserve(per * sizeof(pt_ray));
+            scene->work_hits[k].reserve(per * sizeof(pt_hit));
+            if(tmax) scene->work_tmax[k].reserve(per * sizeof(float));
+            if(stats) scene->work_stats[k].reserve(per * sizeof(pt_ray_stats));
+        }
+        size_t chunks = (count + chunk - 1) / chunk;
+        for(size_t c = 0; c < chunks; c++) {
+            int k = int(c % 3);
+            cudaStream_t st = scene->streams[k];
+            size_t b = c * chunk, n = count - b < chunk ? count - b : chunk;
+            PT_CUDA(cudaMemcpyAsync(scene->work_rays[k].get(), rays + b, n * sizeof(pt_ray), cudaMemcpyHostToDevice, st));
+            if(tmax) PT_CUDA(cudaMemcpyAsync(scene->work_tmax[k].get(), tmax + b, n * sizeof(float), cudaMemcpyHostToDevice, st));
+            launch_query(scene, scene->work_rays[k].get<pt_ray>(), n, mode, tmin, tmax ? scene->work_tmax[k].get<float>() : nullptr,
+                         scene->work_hits[k].get<pt_hit>(), stats ? scene->work_stats[k].get<pt_ray_stats>() : nullptr,
+                         kTieLowestId, st);
+            PT_CUDA(cudaMemcpyAsync(hits + b, scene->work_hits[k].get(), n * sizeof(pt_hit), cudaMemcpyDeviceToHost, st));
+            if(stats) PT_CUDA(cudaMemcpyAsync(stats + b, scene->work_stats[k].get(), n * sizeof(pt_ray_stats), cudaMemcpyDeviceToHost, st));
+        }
+        for(int k = 0; k < 3; k++) PT_CUDA(cudaStreamSynchronize(scene->streams[k]));
+    });
+}
+
+pt_status pt_query_rays_compat(const pt_scene *scene, const pt_ray *rays, size_t count, int brute, pt_trace_result *results) {
+    return guard([&]() {
+        if(!scene || (count && (!rays || !results))) throw Error(PT_INVALID_ARGUMENT, "null argument");
+        if(!count) return;
+        if(count > size_t(INT32_MAX)) throw Error(PT_INVALID_ARGUMENT, "too many validation rays");
+        DeviceBuffer in(count * sizeof(pt_ray)), out(count * sizeof(pt_trace_result));
+        PT_CUDA(cudaMemcpy(in.get(), rays, count * sizeof(pt_ray), cudaMemcpyHostToDevice));
+        compat_kernel<<<grid_for(count, kQueryBlock), kQueryBlock>>>(scene->view, scene->brute_order.get<int32_t>(), scene->leaf_count,
+                                                                     in.get<pt_ray>(), count, brute, out.get<pt_trace_result>());
+        PT_CUDA(cudaGetLastError());
+        PT_CUDA(cudaDeviceSynchronize());
+        PT_CUDA(cudaMemcpy(results, out.get(), count * sizeof(pt_trace_result), cudaMemcpyDeviceToHost));
+    });
+}
+
+pt_status pt_rays_camera_device(const pt_camera *camera, int width, int height, uint64_t seed, uint64_t first,
+                                size_t count, pt_ray *rays, void *stream) {
+    return guard([&]() {
+        if(!camera || (count && !rays) || width <= 0 || height <= 0) throw Error(PT_INVALID_ARGUMENT, "invalid camera ray arguments");
+        if(!count) return;
+        camera_rays_kernel<<<grid_for(count, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(*camera, width, height, seed, first, count, rays);
+        PT_CUDA(cudaGetLastError());
+    });
+}
+
+pt_status pt_rays_bounce_device(const pt_scene *scene, const pt_ray *primary, const pt_hit *hits, size_t count,
+                                uint64_t seed, uint64_t first, pt_ray *out, void *stream) {
+    return guard([&]() {
+        if(!scene || (count && (!primary || !hits || !out))) throw Error(PT_INVALID_ARGUMENT, "null argument");
+        if(!count) return;
+        if(!scene->triangle_count) throw Error(PT_INVALID_ARGUMENT, "bounce rays need triangles");
+        bounce_rays_kernel<<<grid_for(count, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(scene->view, primary, hits, count, seed,
+                                                                                                 first, scene->triangle_count, out);
+        PT_CUDA(cudaGetLastError());
+    });
+}
+
+} // extern "C"

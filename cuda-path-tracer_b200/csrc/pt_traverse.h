@@ -1,0 +1,228 @@
+// pt_traverse.h — closest-hit and any-hit traversal of the re-laid-out BVH (host + device).
+//
+// Semantics follow trace_world (src/renderer/transport.h:43-85):
+//   * boxes are tested over (tmin, limit) with limit = nextafterf(closest, tmax) once a hit
+//     exists, so exact-distance ties stay eligible (transport.h:65-67);
+//   * primitives are tested over (tmin, limit) with the reference's strict bounds;
+//   * overflowing the 64-entry stack sets error = 1 and reports a miss (transport.h:71-72).
+// What differs is the order, which cannot change the answer: both children's boxes are read
+// from the parent (one 64-byte fetch), the nearer passing child is descended first and the
+// other pushed, and leaves are tested as soon as their box passes.  Because every
+// candidate's t is computed bit-identically and boxes are conservative, the set of
+// primitives at the closest distance is independent of the order; among them the winner is
+// picked by a key: the lowest (type, id) (the north-star rule) or, for the compatibility
+// entry point, the last depth-first leaf (the reference's rule, transport.h:76-79).
+#pragma once
+
+#include "pt_exact.h"
+
+namespace ptb {
+
+struct HitInfo {
+    float t, u, v;
+    int32_t slot;   // -1 on a miss
+};
+
+#ifdef __CUDA_ARCH__
+#define PT_LDG4(p) __ldg(reinterpret_cast<const float4 *>(p))
+#define PT_LDGI4(p) __ldg(reinterpret_cast<const int4 *>(p))
+#endif
+
+PT_HD inline long long tie_key(const DeviceScene &s, int32_t slot, int tie) {
+    if (slot < s.tri_slots) {
+        const TriRecord &t = s.tris[slot];
+        return tie == kTieLowestId ? ((1ll << 32) | (uint32_t)t.id) : -(long long)t.node;
+    }
+    const SphereRecord &p = s.spheres[slot - s.tri_slots];
+    return tie == kTieLowestId ? ((2ll << 32) | (uint32_t)p.id) : -(long long)p.node;
+}
+
+PT_HD inline void load_tri(const DeviceScene &s, int32_t slot, TriRecord &t) {
+#ifdef __CUDA_ARCH__
+    const float4 *p = reinterpret_cast<const float4 *>(&s.tris[slot]);
+    float4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2);
+    t.v0x = a.x; t.v0y = a.y; t.v0z = a.z; t.eps = a.w;
+    t.e1x = b.x; t.e1y = b.y; t.e1z = b.z; t.id = __float_as_int(b.w);
+    t.e2x = c.x; t.e2y = c.y; t.e2z = c.z; t.node = __float_as_int(c.w);
+#else
+    t = s.tris[slot];
+#endif
+}
+
+PT_HD inline void load_node(const DeviceScene &s, int32_t node, BvhNode &n) {
+#ifdef __CUDA_ARCH__
+    const float4 *p = reinterpret_cast<const float4 *>(&s.nodes[node]);
+    float4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2);
+    int4 d = __ldg(reinterpret_cast<const int4 *>(p + 3));
+    n.c0lox = a.x; n.c0hix = a.y; n.c0loy = a.z; n.c0hiy = a.w;
+    n.c1lox = b.x; n.c1hix = b.y; n.c1loy = b.z; n.c1hiy = b.w;
+    n.c0loz = c.x; n.c0hiz = c.y; n.c1loz = c.z; n.c1hiz = c.w;
+    n.child0 = d.x; n.child1 = d.y;
+#else
+    n = s.nodes[node];
+#endif
+}
+
+// Tests leaf `slot`; updates the running answer.  Returns true when a hit was accepted.
+template <bool kAny>
+PT_HD inline bool test_leaf(const DeviceScene &s, int32_t slot, const pt_ray &r, float dl, float tmin,
+                            float tmax, int tie, bool &found, float &closest, long long &best_key,
+                            HitInfo &hit, uint32_t &prims) {
+    float limit = found ? nextafterf(closest, tmax) : tmax;
+    float t, u = 0, v = 0;
+    bool ok;
+    prims++;
+    if (slot < s.tri_slots) {
+        if (!(dl > 0)) return false;   // !(direction_length > 0), flat_intersect.h:14
+        TriRecord tr;
+        load_tri(s, slot, tr);
+        ok = tri_hit(tr, r, dl, tmin, limit, t, u, v);
+    } else {
+        SphereRecord sp = s.spheres[slot - s.tri_slots];
+        ok = sphere_hit(sp, r, tmin, limit, t);
+    }
+    if (!ok) return false;
+    if (!kAny && found && !(t < closest)) {
+        long long key = tie_key(s, slot, tie);
+        if (!(key < best_key)) return false;
+        best_key = key;
+    } else if (!kAny) {
+        best_key = tie_key(s, slot, tie);
+    }
+    found = true;
+    closest = t;
+    hit.t = t; hit.u = u; hit.v = v; hit.slot = slot;
+    return true;
+}
+
+// Closest hit (kAny = false) or any hit (kAny = true) over (tmin, tmax).
+template <bool kAny>
+PT_HD inline bool traverse(const DeviceScene &s, const pt_ray &r, float tmin, float tmax, int tie,
+                           HitInfo &hit, uint32_t &boxes, uint32_t &prims, int &error) {
+    hit.slot = -1; hit.t = 0; hit.u = 0; hit.v = 0;
+    if (s.empty || s.node_count == 0) return false;
+    RayBox rb = ray_box(r);
+    float dl = length(mk(r.direction));
+    bool found = false;
+    float closest = tmax;
+    long long best_key = 0;
+    int32_t stack[kStackCapacity];
+    int sp = 0;
+    int32_t node = 0;
+    for (;;) {
+        BvhNode n;
+        load_node(s, node, n);
+        float limit = found ? nextafterf(closest, tmax) : tmax;
+        float e0, e1;
+        bool h0 = n.child0 != kEmptyChild &&
+                  box_hit(rb, n.c0lox, n.c0hix, n.c0loy, n.c0hiy, n.c0loz, n.c0hiz, tmin, limit, e0);
+        bool h1 = n.child1 != kEmptyChild &&
+                  box_hit(rb, n.c1lox, n.c1hix, n.c1loy, n.c1hiy, n.c1loz, n.c1hiz, tmin, limit, e1);
+        boxes += (n.child0 != kEmptyChild) + (n.child1 != kEmptyChild);
+        int32_t first = n.child0, second = n.child1;
+        bool hf = h0, hs = h1;
+        if (h0 && h1 && e1 < e0) { first = n.child1; second = n.child0; }
+        else if (!h0) { first = n.child1; hf = h1; hs = false; }
+        // leaves are tested at once, nearer first
+        int32_t inner[2];
+        int ninner = 0;
+        if (hf) {
+            if (first < 0) {
+                if (test_leaf<kAny>(s, ~first, r, dl, tmin, tmax, tie, found, closest, best_key, hit, prims) && kAny) return true;
+            } else inner[ninner++] = first;
+        }
+        if (hs) {
+            if (second < 0) {
+                if (test_leaf<kAny>(s, ~second, r, dl, tmin, tmax, tie, found, closest, best_key, hit, prims) && kAny) return true;
+            } else inner[ninner++] = second;
+        }
+        if (ninner == 2) {
+            if (sp >= kStackCapacity) { error = 1; hit.slot = -1; return false; }
+            stack[sp++] = inner[1];
+            node = inner[0];
+        } else if (ninner == 1) {
+            node = inner[0];
+        } else {
+            if (sp == 0) break;
+            node = stack[--sp];
+        }
+    }
+    return found;
+}
+
+// trace_world(…, brute = true) (src/renderer/transport.h:48-60): every leaf, in flat
+// node-array order, without pruning.
+template <bool kAny>
+PT_HD inline bool traverse_brute(const DeviceScene &s, const int32_t *order, int32_t leaves, const pt_ray &r,
+                                 float tmin, float tmax, int tie, HitInfo &hit, uint32_t &prims) {
+    hit.slot = -1; hit.t = 0; hit.u = 0; hit.v = 0;
+    if (s.empty) return false;
+    float dl = length(mk(r.direction));
+    bool found = false;
+    float closest = tmax;
+    long long best_key = 0;
+    for (int32_t i = 0; i < leaves; i++) {
+        if (test_leaf<kAny>(s, order[i], r, dl, tmin, tmax, tie, found, closest, best_key, hit, prims) && kAny)
+            return true;
+    }
+    return found;
+}
+
+// ---- full hit record of the winner (src/flat/flat_intersect.h:27-42, 53-64) ----
+PT_HD inline void sphere_uv(f3 p, float &u, float &v) {
+    // get_sphere_uv, src/geometry/sphere_uv.h:7-13: atan2/asin on float, the rest in double
+    const double pi = 3.14159265358979323846;
+    float phi = atan2f(p.z, p.x);
+    float theta = asinf(p.y);
+    u = (float)(1 - ((double)phi + pi) / (2 * pi));
+    v = (float)(((double)theta + pi / 2) / pi);
+}
+
+PT_HD inline void finalize_hit(const DeviceScene &s, const pt_ray &r, const HitInfo &h, pt_flat_hit &rec) {
+    f3 o = mk(r.origin), d = mk(r.direction);
+    rec.t = h.t;
+    f3 p = o + h.t * d;
+    rec.p = pv(p);
+    if (h.slot < s.tri_slots) {
+        const TriRecord &tr = s.tris[h.slot];
+        const pt_triangle &face = s.triangles[tr.id];
+        float u = h.u, v = h.v;
+        f3 edge1 = mk(face.v1) - mk(face.v0), edge2 = mk(face.v2) - mk(face.v0);
+        f3 outward = cross(edge1, edge2);
+        float normal_length = length(outward);
+        outward = div_assign(outward, normal_length);
+        f3 normal = outward;
+        if (face.smooth) {
+            f3 interpolated = (1 - u - v) * mk(face.n0) + u * mk(face.n1) + v * mk(face.n2);
+            float length_squared = sqlen(interpolated);
+            if (length_squared > 0 && finite(length_squared)) {
+                normal = unit(interpolated);
+                if (dot(normal, outward) < 0) normal = -normal;
+                if (dot(normal, outward) == 0) normal = outward;
+            }
+        }
+        rec.normal = pv(normal);
+        f3 uv = (1 - u - v) * mk(face.uv0) + u * mk(face.uv1) + v * mk(face.uv2);
+        rec.u = uv.x; rec.v = uv.y;
+        rec.material_id = face.material_id;
+        rec.primitive_type = PT_TRIANGLE;
+        rec.primitive_id = tr.id;
+    } else {
+        const SphereRecord &sr = s.spheres[h.slot - s.tri_slots];
+        const pt_sphere &sp = s.sphere_src[sr.id];
+        f3 normal = (p - mk(sp.center)) / sp.radius;
+        rec.normal = pv(normal);
+        sphere_uv(normal, rec.u, rec.v);
+        rec.material_id = sp.material_id;
+        rec.primitive_type = PT_SPHERE;
+        rec.primitive_id = sr.id;
+    }
+}
+
+PT_HD inline void hit_ids(const DeviceScene &s, int32_t slot, int32_t &type, int32_t &id) {
+    if (slot < 0) { type = PT_BRANCH; id = -1; return; }
+    if (slot < s.tri_slots) { type = PT_TRIANGLE; id = s.tris[slot].id; return; }
+    type = PT_SPHERE; id = s.spheres[slot - s.tri_slots].id;
+}
+
+} // namespace ptb

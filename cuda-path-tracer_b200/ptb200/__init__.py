@@ -1,0 +1,370 @@
+"""ptb200 — Python binding of the B200 path-tracing core (libptb200.so, C ABI in include/pt.h).
+
+Mirrors the reference renderer surface of AdmiralHeathCL/cuda-path-tracer:
+
+* ``cuda_device_available()``            — src/cuda/cuda_renderer.h:8
+* ``CudaRenderer``                        — class cuda_renderer, src/cuda/cuda_renderer.h:10-29
+* ``cuda_query_rays(scene, rays, brute)`` — src/cuda/cuda_renderer.h:32
+* numpy record dtypes with the byte layout of the flat transfer records (src/flat/flat_data.h).
+
+Errors raise the exception types the reference throws: ``ValueError`` for its
+``std::invalid_argument`` and ``RuntimeError`` for its ``std::runtime_error``.  There is no
+CPU fallback: without the compiled library or a CUDA device every call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+_HERE = Path(__file__).resolve().parent
+LIBRARY_PATH = _HERE.parent / "libptb200.so"
+
+# ---------------------------------------------------------------- record dtypes (pt.h)
+VEC3 = ("<f4", (3,))
+TRIANGLE = np.dtype([("v0", *VEC3), ("v1", *VEC3), ("v2", *VEC3), ("n0", *VEC3), ("n1", *VEC3), ("n2", *VEC3),
+                     ("uv0", *VEC3), ("uv1", *VEC3), ("uv2", *VEC3), ("material_id", "<i4"), ("smooth", "<i4")])
+SPHERE = np.dtype([("center", *VEC3), ("radius", "<f4"), ("material_id", "<i4")])
+NODE = np.dtype([("minimum", *VEC3), ("maximum", *VEC3), ("type", "<i4"), ("left", "<i4"), ("right", "<i4"),
+                 ("primitive", "<i4")])
+MATERIAL = np.dtype([("albedo", *VEC3), ("fuzz", "<f4"), ("ref_idx", "<f4"), ("type", "<i4"), ("texture_id", "<i4")])
+TEXTURE = np.dtype([("color", *VEC3), ("scale", *VEC3), ("offset", *VEC3), ("type", "<i4"), ("image_id", "<i4"),
+                    ("width", "<i4"), ("height", "<i4"), ("byte_offset", "<i4"), ("clamp", "<i4")])
+CAMERA = np.dtype([("origin", *VEC3), ("lower_left_corner", *VEC3), ("horizontal", *VEC3), ("vertical", *VEC3),
+                   ("u", *VEC3), ("v", *VEC3), ("lens_radius", "<f4"), ("time0", "<f4"), ("time1", "<f4")])
+RAY = np.dtype([("origin", *VEC3), ("direction", *VEC3), ("time", "<f4")])
+FLAT_HIT = np.dtype([("t", "<f4"), ("u", "<f4"), ("v", "<f4"), ("p", *VEC3), ("normal", *VEC3),
+                     ("material_id", "<i4"), ("primitive_type", "<i4"), ("primitive_id", "<i4")])
+TRACE_RESULT = np.dtype([("rec", FLAT_HIT), ("hit", "<i4"), ("error", "<i4")])
+LIGHT = np.dtype([("type", "<i4"), ("primitive", "<i4"), ("cumulative_area", "<f4")])
+HIT = np.dtype([("t", "<f4"), ("primitive_id", "<i4"), ("primitive_type", "<i4"), ("error", "<i4")])
+RAY_STATS = np.dtype([("boxes", "<u4"), ("primitives", "<u4")])
+for _name, _dt, _size in [("triangle", TRIANGLE, 116), ("sphere", SPHERE, 20), ("node", NODE, 40),
+                          ("material", MATERIAL, 28), ("texture", TEXTURE, 60), ("camera", CAMERA, 84),
+                          ("ray", RAY, 28), ("flat_hit", FLAT_HIT, 48), ("trace_result", TRACE_RESULT, 56),
+                          ("light", LIGHT, 12), ("hit", HIT, 16)]:
+    assert _dt.itemsize == _size, (_name, _dt.itemsize)
+
+BRANCH, TRIANGLE_TYPE, SPHERE_TYPE = 0, 1, 2
+DIFFUSE, METAL, GLASS, LIGHT_MAT = 0, 1, 2, 3
+TEX_CONSTANT, TEX_IMAGE, TEX_MAP = 0, 1, 2
+DEBUG_SHADED, DEBUG_NORMALS, DEBUG_TRIANGLE, DEBUG_MATERIAL, DEBUG_BVH, DEBUG_INTERSECTIONS = range(6)
+QUERY_CLOSEST, QUERY_ANY = 0, 1
+RENDER_MIS, RENDER_BRUTE = 1, 2
+
+STATUS = {0: "PT_OK", 1: "PT_INVALID_ARGUMENT", 2: "PT_INVALID_SCENE", 3: "PT_CUDA_ERROR",
+          4: "PT_STACK_OVERFLOW", 5: "PT_QUEUE_OVERFLOW", 6: "PT_TIMEOUT", 7: "PT_NO_DEVICE"}
+
+
+class PtError(RuntimeError):
+    """A failing pt_* call; ``status`` is the pt_status code."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS.get(status, status)}: {message}")
+        self.status = status
+
+
+class PtInvalidArgument(PtError, ValueError):
+    """PT_INVALID_ARGUMENT — the reference's std::invalid_argument."""
+
+
+class _SceneDesc(C.Structure):
+    _fields_ = [("triangles", C.c_void_p), ("triangle_count", C.c_size_t),
+                ("spheres", C.c_void_p), ("sphere_count", C.c_size_t),
+                ("nodes", C.c_void_p), ("node_count", C.c_size_t),
+                ("materials", C.c_void_p), ("material_count", C.c_size_t),
+                ("textures", C.c_void_p), ("texture_count", C.c_size_t),
+                ("pixels", C.c_void_p), ("pixel_bytes", C.c_size_t),
+                ("root", C.c_int32), ("max_depth", C.c_int32)]
+
+
+class ProceduralParams(C.Structure):
+    """pt_procedural_params (include/pt_workloads.h)."""
+    _fields_ = [("sphere_count", C.c_int), ("segments", C.c_int), ("rings", C.c_int), ("box_size", C.c_float),
+                ("displacement", C.c_float), ("radius_min", C.c_float), ("radius_max", C.c_float),
+                ("floor", C.c_int), ("light_fraction", C.c_float), ("light_radiance", C.c_float),
+                ("metal_fraction", C.c_float), ("glass_fraction", C.c_float), ("seed", C.c_uint64),
+                ("random_triangles", C.c_int), ("soup_edge_min", C.c_float), ("soup_edge_max", C.c_float)]
+
+
+_lib = None
+
+
+def library() -> C.CDLL:
+    """Loads libptb200.so (built by __graft_entry__.build() / make -C cuda-path-tracer_b200)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIBRARY_PATH.exists():
+        raise RuntimeError(f"libptb200.so is not built ({LIBRARY_PATH}); run make -C cuda-path-tracer_b200")
+    lib = C.CDLL(str(LIBRARY_PATH))
+    P, S, I, U64, F = C.c_void_p, C.c_size_t, C.c_int, C.c_uint64, C.c_float
+    sig = {
+        "pt_device_available": (I, [C.c_char_p, S]),
+        "pt_last_error": (C.c_char_p, []),
+        "pt_abi_version": (I, []),
+        "pt_scene_create": (I, [P, P]),
+        "pt_scene_destroy": (I, [P]),
+        "pt_scene_lights": (I, [P, P, S, P, P]),
+        "pt_scene_device_bytes": (I, [P, P]),
+        "pt_query_rays_device": (I, [P, P, S, I, F, P, P, P, P]),
+        "pt_query_rays_brute_device": (I, [P, P, S, I, F, P, P, P, P]),
+        "pt_query_rays": (I, [P, P, S, I, F, P, P, P]),
+        "pt_query_rays_compat": (I, [P, P, S, I, P]),
+        "pt_rays_camera_device": (I, [P, I, I, U64, U64, S, P, P]),
+        "pt_rays_bounce_device": (I, [P, P, P, S, U64, U64, P, P]),
+        "pt_flat_from_desc": (I, [P, P]),
+        "pt_flat_build_bvh": (I, [P, I]),
+        "pt_flat_desc": (I, [P, P]),
+        "pt_flat_destroy": (I, [P]),
+        "pt_make_camera": (I, [P, P, P, F, F, F, F, F, F, P]),
+        "pt_workload_cornell": (I, [I, I, P, P]),
+        "pt_procedural_defaults": (None, [P]),
+        "pt_workload_procedural": (I, [P, I, I, P, P]),
+        "pt_rays_camera": (I, [P, I, I, U64, U64, S, P]),
+        "pt_rays_surface": (I, [P, U64, U64, S, P, P, I]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(status: int) -> None:
+    if status != 0:
+        msg = library().pt_last_error().decode(errors="replace")
+        if status == 1:
+            raise PtInvalidArgument(status, msg)
+        raise PtError(status, msg)
+
+
+def _ptr(a) -> int | None:
+    """Address of a numpy array, a torch tensor, an int address or None."""
+    if a is None:
+        return None
+    if isinstance(a, int):
+        return a
+    if isinstance(a, np.ndarray):
+        assert a.flags["C_CONTIGUOUS"], "arrays must be contiguous"
+        return a.ctypes.data
+    if hasattr(a, "data_ptr"):
+        return a.data_ptr()
+    raise TypeError(f"cannot take the address of {type(a)!r}")
+
+
+def cuda_device_available() -> tuple[bool, str]:
+    """cuda_device_available(description) (src/cuda/cuda_renderer.cu:128-140)."""
+    buf = C.create_string_buffer(256)
+    ok = library().pt_device_available(buf, 256)
+    return bool(ok), buf.value.decode(errors="replace")
+
+
+# ---------------------------------------------------------------- host flat scenes
+class FlatScene:
+    """Host flat scene (the reference's ``flat_scene``): numpy arrays of the transfer records."""
+
+    def __init__(self, triangles=None, spheres=None, nodes=None, materials=None, textures=None, pixels=None,
+                 root=-1, max_depth=0):
+        self.triangles = np.ascontiguousarray(triangles if triangles is not None else np.zeros(0, TRIANGLE), TRIANGLE)
+        self.spheres = np.ascontiguousarray(spheres if spheres is not None else np.zeros(0, SPHERE), SPHERE)
+        self.nodes = np.ascontiguousarray(nodes if nodes is not None else np.zeros(0, NODE), NODE)
+        self.materials = np.ascontiguousarray(materials if materials is not None else np.zeros(0, MATERIAL), MATERIAL)
+        self.textures = np.ascontiguousarray(textures if textures is not None else np.zeros(0, TEXTURE), TEXTURE)
+        self.pixels = np.ascontiguousarray(pixels if pixels is not None else np.zeros(0, np.uint8), np.uint8)
+        self.root = int(root)
+        self.max_depth = int(max_depth)
+
+    def desc(self) -> _SceneDesc:
+        d = _SceneDesc()
+        for name in ("triangles", "spheres", "nodes", "materials", "textures", "pixels"):
+            arr = getattr(self, name)
+            setattr(d, name, arr.ctypes.data if arr.size else None)
+        d.triangle_count, d.sphere_count, d.node_count = len(self.triangles), len(self.spheres), len(self.nodes)
+        d.material_count, d.texture_count, d.pixel_bytes = len(self.materials), len(self.textures), len(self.pixels)
+        d.root, d.max_depth = self.root, self.max_depth
+        return d
+
+    def copy(self) -> "FlatScene":
+        return FlatScene(self.triangles.copy(), self.spheres.copy(), self.nodes.copy(), self.materials.copy(),
+                         self.textures.copy(), self.pixels.copy(), self.root, self.max_depth)
+
+    def build_bvh(self, threads: int = 0) -> "FlatScene":
+        """Replaces the nodes with the library's binned-SAH tree (pt_flat_build_bvh)."""
+        lib = library()
+        h = C.c_void_p()
+        d = self.desc()
+        check(lib.pt_flat_from_desc(C.byref(d), C.byref(h)))
+        try:
+            check(lib.pt_flat_build_bvh(h, threads))
+            return _flat_from_handle(h)
+        finally:
+            lib.pt_flat_destroy(h)
+
+    def save(self, path) -> None:
+        np.savez_compressed(path, triangles=self.triangles, spheres=self.spheres, nodes=self.nodes,
+                            materials=self.materials, textures=self.textures, pixels=self.pixels,
+                            root=self.root, max_depth=self.max_depth)
+
+    @staticmethod
+    def load(path) -> "FlatScene":
+        z = np.load(path)
+        return FlatScene(z["triangles"], z["spheres"], z["nodes"], z["materials"], z["textures"], z["pixels"],
+                         int(z["root"]), int(z["max_depth"]))
+
+
+def _flat_from_handle(h) -> FlatScene:
+    d = _SceneDesc()
+    check(library().pt_flat_desc(h, C.byref(d)))
+
+    def grab(ptr, count, dtype):
+        out = np.zeros(count, dtype)
+        if count:
+            C.memmove(out.ctypes.data, ptr, count * dtype.itemsize)
+        return out
+    return FlatScene(grab(d.triangles, d.triangle_count, TRIANGLE), grab(d.spheres, d.sphere_count, SPHERE),
+                     grab(d.nodes, d.node_count, NODE), grab(d.materials, d.material_count, MATERIAL),
+                     grab(d.textures, d.texture_count, TEXTURE), grab(d.pixels, d.pixel_bytes, np.dtype(np.uint8)),
+                     d.root, d.max_depth)
+
+
+def make_camera(lookfrom, lookat, vup=(0, 1, 0), vfov=40.0, aspect=1.0, aperture=0.0, focus_dist=1.0,
+                time0=0.0, time1=1.0) -> np.ndarray:
+    """The reference camera (src/core/camera.h:16-43), flattened."""
+    out = np.zeros(1, CAMERA)
+    f = lambda v: (C.c_float * 3)(*v)
+    check(library().pt_make_camera(f(lookfrom), f(lookat), f(vup), vfov, aspect, aperture, focus_dist, time0, time1,
+                                   out.ctypes.data))
+    return out
+
+
+def cornell_box(width: int = 320, height: int = 200) -> tuple[FlatScene, np.ndarray]:
+    """The 20-triangle Cornell-style box with three spheres (pt_workload_cornell)."""
+    lib = library()
+    h = C.c_void_p()
+    cam = np.zeros(1, CAMERA)
+    check(lib.pt_workload_cornell(width, height, C.byref(h), cam.ctypes.data))
+    try:
+        return _flat_from_handle(h), cam
+    finally:
+        lib.pt_flat_destroy(h)
+
+
+def procedural_params(**overrides) -> ProceduralParams:
+    p = ProceduralParams()
+    library().pt_procedural_defaults(C.byref(p))
+    for k, v in overrides.items():
+        setattr(p, k, v)
+    return p
+
+
+def procedural_scene(width: int = 960, height: int = 600, **overrides) -> tuple[FlatScene, np.ndarray]:
+    """Displaced-sphere scene (pt_workload_procedural); defaults = the 1M-triangle scene."""
+    lib = library()
+    p = procedural_params(**overrides)
+    h = C.c_void_p()
+    cam = np.zeros(1, CAMERA)
+    check(lib.pt_workload_procedural(C.byref(p), width, height, C.byref(h), cam.ctypes.data))
+    try:
+        return _flat_from_handle(h), cam
+    finally:
+        lib.pt_flat_destroy(h)
+
+
+def camera_rays(camera: np.ndarray, width: int, height: int, seed: int, first: int, count: int) -> np.ndarray:
+    out = np.zeros(count, RAY)
+    check(library().pt_rays_camera(camera.ctypes.data, width, height, seed, first, count, out.ctypes.data))
+    return out
+
+
+def surface_rays(scene: FlatScene, seed: int, first: int, count: int, shadow: bool = False, threads: int = 0):
+    lib = library()
+    h = C.c_void_p()
+    d = scene.desc()
+    check(lib.pt_flat_from_desc(C.byref(d), C.byref(h)))
+    try:
+        rays = np.zeros(count, RAY)
+        tmax = np.zeros(count, np.float32) if shadow else None
+        check(lib.pt_rays_surface(h, seed, first, count, rays.ctypes.data, _ptr(tmax), threads))
+        return (rays, tmax) if shadow else rays
+    finally:
+        lib.pt_flat_destroy(h)
+
+
+# ---------------------------------------------------------------- device scene + queries
+class Scene:
+    """Device-resident scene (pt_scene_create): validated, re-laid out and uploaded."""
+
+    def __init__(self, flat: FlatScene):
+        self.flat = flat
+        self._h = C.c_void_p()
+        d = flat.desc()
+        check(library().pt_scene_create(C.byref(d), C.byref(self._h)))
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            library().pt_scene_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def lights(self):
+        n = C.c_size_t()
+        area = C.c_float()
+        check(library().pt_scene_lights(self._h, None, 0, C.byref(n), C.byref(area)))
+        out = np.zeros(n.value, LIGHT)
+        check(library().pt_scene_lights(self._h, _ptr(out), n.value, C.byref(n), C.byref(area)))
+        return out, area.value
+
+    def device_bytes(self) -> int:
+        n = C.c_size_t()
+        check(library().pt_scene_device_bytes(self._h, C.byref(n)))
+        return n.value
+
+    def query(self, rays: np.ndarray, mode: int = QUERY_CLOSEST, tmin: float = 0.001, tmax=None, stats=False):
+        """Host-buffer query (pt_query_rays): returns HIT records (and RAY_STATS)."""
+        rays = np.ascontiguousarray(rays, RAY)
+        hits = np.zeros(len(rays), HIT)
+        st = np.zeros(len(rays), RAY_STATS) if stats else None
+        tm = None if tmax is None else np.ascontiguousarray(tmax, np.float32)
+        check(library().pt_query_rays(self._h, _ptr(rays), len(rays), mode, tmin, _ptr(tm), _ptr(hits), _ptr(st)))
+        return (hits, st) if stats else hits
+
+    def query_device(self, rays, count: int, hits, mode: int = QUERY_CLOSEST, tmin: float = 0.001, tmax=None,
+                     stats=None, stream=0, brute=False):
+        """Device-buffer query (pt_query_rays_device); arguments are device addresses or tensors."""
+        fn = library().pt_query_rays_brute_device if brute else library().pt_query_rays_device
+        check(fn(self._h, _ptr(rays), count, mode, tmin, _ptr(tmax), _ptr(hits), _ptr(stats), stream))
+
+    def query_compat(self, rays: np.ndarray, brute: bool = False) -> np.ndarray:
+        rays = np.ascontiguousarray(rays, RAY)
+        out = np.zeros(len(rays), TRACE_RESULT)
+        check(library().pt_query_rays_compat(self._h, _ptr(rays), len(rays), int(brute), _ptr(out)))
+        return out
+
+    def bounce_rays_device(self, primary, hits, count: int, seed: int, first: int, out, stream=0):
+        check(library().pt_rays_bounce_device(self._h, _ptr(primary), _ptr(hits), count, seed, first, _ptr(out), stream))
+
+
+def camera_rays_device(camera: np.ndarray, width, height, seed, first, count, out, stream=0):
+    check(library().pt_rays_camera_device(camera.ctypes.data, width, height, seed, first, count, _ptr(out), stream))
+
+
+def cuda_query_rays(scene: FlatScene, rays: np.ndarray, brute: bool = False) -> np.ndarray:
+    """cuda_query_rays(scene, rays, brute) (src/cuda/cuda_renderer.cu:248-260): TRACE_RESULT records."""
+    s = Scene(scene)
+    try:
+        return s.query_compat(rays, brute)
+    finally:
+        s.close()

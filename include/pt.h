@@ -1,0 +1,190 @@
+/*
+ * pt.h — C ABI of the B200 path-tracing core.
+ *
+ * Drop-in boundary for the reference renderer surface of
+ * AdmiralHeathCL/cuda-path-tracer:
+ *   - `cuda_device_available`           src/cuda/cuda_renderer.h:8
+ *   - `class cuda_renderer`             src/cuda/cuda_renderer.h:10-29
+ *   - `cuda_query_rays`                 src/cuda/cuda_renderer.h:32
+ *   - the flat transfer records         src/flat/flat_data.h:10-62
+ *   - `ray`                             src/core/ray.h:6-33
+ *   - `trace_result`                    src/renderer/transport.h:12
+ *
+ * Every record below has the byte layout of the reference record it names,
+ * so `flat_scene` vectors can be handed over with `.data()` / `.size()`.
+ * No function allocates on behalf of the caller except the opaque handles
+ * it returns; every handle owns its device memory and is released by the
+ * matching destroy call.  Functions return a pt_status; the message of the
+ * last failure on the calling thread is available from pt_last_error().
+ */
+#ifndef PT_B200_H
+#define PT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PT_ABI_VERSION 1
+
+/* ---- status codes (the C++ wrapper maps them to the reference's exception types) ---- */
+typedef enum pt_status {
+    PT_OK = 0,
+    PT_INVALID_ARGUMENT = 1, /* std::invalid_argument in the reference (bad dims, sample counts, block shapes) */
+    PT_INVALID_SCENE = 2,    /* std::runtime_error("invalid flat scene data"), src/flat/flat_validate.h:12 */
+    PT_CUDA_ERROR = 3,       /* std::runtime_error from a failing CUDA call, src/cuda/cuda_renderer.cu:8-11 */
+    PT_STACK_OVERFLOW = 4,   /* "CUDA traversal stack overflow", src/cuda/cuda_renderer.cu:204 */
+    PT_QUEUE_OVERFLOW = 5,   /* a wavefront queue would exceed its capacity */
+    PT_TIMEOUT = 6,          /* a bounded device-side wait ran out */
+    PT_NO_DEVICE = 7         /* cuda_device_available() == false; the CLI exits 77 */
+} pt_status;
+
+/* ---- enums, same values as src/flat/flat_data.h:10-12 and src/renderer/transport.h:10 ---- */
+enum { PT_BRANCH = 0, PT_TRIANGLE = 1, PT_SPHERE = 2 };
+enum { PT_DIFFUSE = 0, PT_METAL = 1, PT_GLASS = 2, PT_LIGHT = 3 };
+enum { PT_TEX_CONSTANT = 0, PT_TEX_IMAGE = 1, PT_TEX_MAP = 2 };
+enum { PT_DEBUG_SHADED = 0, PT_DEBUG_NORMALS = 1, PT_DEBUG_TRIANGLE = 2, PT_DEBUG_MATERIAL = 3,
+       PT_DEBUG_BVH = 4, PT_DEBUG_INTERSECTIONS = 5 };
+
+/* ---- transfer records (byte-compatible with the reference) ---- */
+typedef struct pt_vec3 { float x, y, z; } pt_vec3;                       /* vec3, src/core/vec3.h:9 */
+typedef struct pt_triangle {                                              /* flat_triangle, 116 B */
+    pt_vec3 v0, v1, v2, n0, n1, n2, uv0, uv1, uv2;
+    int32_t material_id, smooth;
+} pt_triangle;
+typedef struct pt_sphere { pt_vec3 center; float radius; int32_t material_id; } pt_sphere; /* flat_sphere, 20 B */
+typedef struct pt_node {                                                  /* flat_node, 40 B */
+    pt_vec3 minimum, maximum;
+    int32_t type, left, right, primitive;
+} pt_node;
+typedef struct pt_material { pt_vec3 albedo; float fuzz, ref_idx; int32_t type, texture_id; } pt_material; /* 28 B */
+typedef struct pt_texture {                                               /* flat_texture, 60 B */
+    pt_vec3 color, scale, offset;
+    int32_t type, image_id, width, height, byte_offset, clamp;
+} pt_texture;
+typedef struct pt_camera {                                                /* flat_camera, 84 B */
+    pt_vec3 origin, lower_left_corner, horizontal, vertical, u, v;
+    float lens_radius, time0, time1;
+} pt_camera;
+typedef struct pt_ray { pt_vec3 origin, direction; float time; } pt_ray;  /* ray, 28 B */
+typedef struct pt_flat_hit {                                              /* flat_hit, 48 B */
+    float t, u, v;
+    pt_vec3 p, normal;
+    int32_t material_id, primitive_type, primitive_id;
+} pt_flat_hit;
+typedef struct pt_trace_result { pt_flat_hit rec; int32_t hit, error; } pt_trace_result; /* trace_result, 56 B */
+typedef struct pt_light { int32_t type, primitive; float cumulative_area; } pt_light;     /* flat_light, 12 B */
+
+/* Compact per-ray answer of pt_query_rays (16 B, one vector store per ray).
+ * primitive_type is PT_BRANCH (0) on a miss.  For any-hit queries t is the
+ * distance of the first occluder found (not necessarily the closest). */
+typedef struct pt_hit { float t; int32_t primitive_id; int32_t primitive_type; int32_t error; } pt_hit;
+/* Per-ray traversal counters: child boxes tested and primitives tested. */
+typedef struct pt_ray_stats { uint32_t boxes, primitives; } pt_ray_stats;
+
+/* Scene input: the arrays of a reference `flat_scene` (src/flat/flat_data.h:53-62). */
+typedef struct pt_scene_desc {
+    const pt_triangle *triangles; size_t triangle_count;
+    const pt_sphere *spheres;     size_t sphere_count;
+    const pt_node *nodes;         size_t node_count;
+    const pt_material *materials; size_t material_count;
+    const pt_texture *textures;   size_t texture_count;
+    const unsigned char *pixels;  size_t pixel_bytes;
+    int32_t root;                 /* -1 for an empty scene */
+    int32_t max_depth;            /* depth of the tree, root = 1; checked like validate_flat_scene */
+} pt_scene_desc;
+
+typedef struct pt_scene pt_scene;       /* device-resident scene (BVH re-laid out, lights table) */
+typedef struct pt_renderer pt_renderer; /* progressive renderer state (sums, PCG states, queues) */
+
+/* ---- device probe ----
+ * Replaces bool cuda_device_available(std::string&), src/cuda/cuda_renderer.cu:128-140.
+ * Writes the device name (or the reason it is unavailable) into `description`. */
+int pt_device_available(char *description, size_t capacity);
+const char *pt_last_error(void);
+int pt_abi_version(void);
+
+/* ---- scene ----
+ * Replaces the device_scene upload inside cuda_renderer/cuda_query_rays
+ * (src/cuda/cuda_renderer.cu:36-54, 177-183, 248-260): validates with the rules of
+ * validate_flat_scene (src/flat/flat_validate.h:10-83), builds the emitter table
+ * (scene_lights, src/renderer/scene_view.h:10-28), re-lays the BVH out as 64-byte
+ * two-child nodes and the triangles as 48-byte {v0, e1, e2} records, and uploads.
+ * The caller's arrays may be freed once this returns. */
+pt_status pt_scene_create(const pt_scene_desc *desc, pt_scene **out);
+pt_status pt_scene_destroy(pt_scene *scene);
+/* Emitter table as built on the host (count, then up to `capacity` records). */
+pt_status pt_scene_lights(const pt_scene *scene, pt_light *lights, size_t capacity, size_t *count, float *total_area);
+/* Device bytes held by the scene (nodes, triangles, shading records, lights). */
+pt_status pt_scene_device_bytes(const pt_scene *scene, size_t *bytes);
+
+/* ---- ray queries ----
+ * Closest hit follows trace_world(…, brute=false) (src/renderer/transport.h:43-85) with
+ * exact-distance ties resolved to the lowest (primitive_type, primitive_id); any-hit answers
+ * whether a primitive is hit in (tmin, tmax), the question trace_color's shadow query asks
+ * (src/renderer/transport.h:206-209). */
+enum { PT_QUERY_CLOSEST = 0, PT_QUERY_ANY = 1 };
+/* Device buffers, asynchronous on `stream` (a cudaStream_t; 0 = legacy default stream).
+ * `tmax` may be NULL (FLT_MAX for every ray); `stats` may be NULL. */
+pt_status pt_query_rays_device(const pt_scene *scene, const pt_ray *rays, size_t count, int mode,
+                               float tmin, const float *tmax, pt_hit *hits, pt_ray_stats *stats,
+                               void *stream);
+/* Host buffers: uploads, traces and downloads in overlapped chunks; returns when `hits` is filled. */
+pt_status pt_query_rays(const pt_scene *scene, const pt_ray *rays, size_t count, int mode,
+                        float tmin, const float *tmax, pt_hit *hits, pt_ray_stats *stats);
+/* Compatibility form of cuda_query_rays(scene, rays, brute) (src/cuda/cuda_renderer.cu:248-260):
+ * host rays in, full 56-byte trace_result records out, t range (0.001, FLT_MAX).
+ * brute != 0 scans every leaf in node-array order (src/renderer/transport.h:48-60). */
+pt_status pt_query_rays_compat(const pt_scene *scene, const pt_ray *rays, size_t count, int brute,
+                               pt_trace_result *results);
+/* trace_world(…, brute = true) (src/renderer/transport.h:48-60): every leaf in node-array order,
+ * no pruning, same answer and tie rule as pt_query_rays_device.  Device buffers. */
+pt_status pt_query_rays_brute_device(const pt_scene *scene, const pt_ray *rays, size_t count, int mode,
+                                     float tmin, const float *tmax, pt_hit *hits, pt_ray_stats *stats,
+                                     void *stream);
+
+/* ---- device ray generators (bit-identical to the host ones in pt_workloads.h) ----
+ * Camera rays of pt_rays_camera; bounce rays from closest hits: origin at the hit, a
+ * cosine-distributed direction about the geometric normal turned toward the ray, one PCG stream
+ * per ray seeded (seed, first + k); a primary miss becomes a random surface ray. */
+pt_status pt_rays_camera_device(const pt_camera *camera, int width, int height, uint64_t seed, uint64_t first,
+                                size_t count, pt_ray *rays, void *stream);
+pt_status pt_rays_bounce_device(const pt_scene *scene, const pt_ray *primary, const pt_hit *hits, size_t count,
+                                uint64_t seed, uint64_t first, pt_ray *rays, void *stream);
+
+/* ---- progressive renderer ----
+ * Replaces class cuda_renderer (src/cuda/cuda_renderer.h:10-29).  `flags` is a bit set of
+ * PT_RENDER_*; `max_depth` is the last bounce index of trace_color's loop (the reference
+ * hard-codes 50, src/renderer/transport.h:174,193). */
+enum { PT_RENDER_MIS = 1, PT_RENDER_BRUTE = 2 };
+pt_status pt_renderer_create(const pt_scene *scene, const pt_camera *camera, int width, int height,
+                             uint64_t seed, uint32_t flags, int debug_mode, int max_depth,
+                             pt_renderer **out);
+pt_status pt_renderer_destroy(pt_renderer *renderer);
+/* reset(camera): zero the sums, reseed every pixel's PCG stream (src/cuda/cuda_renderer.cu:186-194). */
+pt_status pt_reset(pt_renderer *renderer, const pt_camera *camera);
+/* add_samples(count) (src/cuda/cuda_renderer.cu:196-213); blocks until the samples are done. */
+pt_status pt_add_samples(pt_renderer *renderer, int count);
+/* set_block_shape(w, h): accepted shapes 8x8, 16x8, 16x16, 32x8 (src/cuda/cuda_renderer.cu:215-228).
+ * Sets the thread-block size of the wavefront kernels to w*h threads. */
+pt_status pt_set_block_shape(pt_renderer *renderer, int width, int height);
+/* Linear FP32 radiance sums (3 floats per pixel, row 0 at the bottom, not divided by spp). */
+pt_status pt_get_sums(const pt_renderer *renderer, float *rgb_sums, size_t floats);
+/* image(): sums / spp (src/cuda/cuda_renderer.cu:230-234). */
+pt_status pt_get_image(const pt_renderer *renderer, float *rgb, size_t floats);
+/* Per-pixel PCG-XSH-RR states as (state, increment) pairs (src/renderer/random.h:8-23). */
+pt_status pt_get_rng(const pt_renderer *renderer, uint64_t *state_increment_pairs, size_t words);
+/* write_rgba(device_ptr, bytes): gamma-2 RGBA8 packing (src/cuda/cuda_renderer.cu:99-109, 235-240). */
+pt_status pt_write_rgba(const pt_renderer *renderer, unsigned char *device_pixels, size_t bytes);
+/* rgba_image(): same bytes, into host memory. */
+pt_status pt_rgba_image(const pt_renderer *renderer, unsigned char *host_pixels, size_t bytes);
+/* sample_count(), kernel_milliseconds(), rays_traced(). */
+pt_status pt_stats(const pt_renderer *renderer, int *samples, float *kernel_ms, uint64_t *rays);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,75 @@
+/*
+ * pt_workloads.h — host-side scene tools of the B200 path-tracing core.
+ *
+ * The reference builds scenes from OBJ/MTL through its own pointer BVH and flattens them
+ * (src/bvh/bvh.h:132-171, src/flat/flat_export.h:13-124); these entry points produce the same
+ * flat format for the benchmark workloads, with a binned-SAH tree in place of the random
+ * median split.  They need no GPU.  Ray generators that must agree bit-for-bit between host
+ * and device use only +, -, *, / and sqrt (no transcendental functions).
+ */
+#ifndef PT_B200_WORKLOADS_H
+#define PT_B200_WORKLOADS_H
+
+#include "pt.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct pt_flat pt_flat; /* host-owned flat scene (the reference's flat_scene) */
+
+/* Copies the arrays of `desc`; nodes/root/max_depth are kept as given. */
+pt_status pt_flat_from_desc(const pt_scene_desc *desc, pt_flat **out);
+/* Replaces the node array with a binned-SAH tree over all triangles and spheres
+ * (one primitive per leaf, preorder, padded triangle bounds, depth <= 64). threads <= 0: all. */
+pt_status pt_flat_build_bvh(pt_flat *scene, int threads);
+/* Pointers into the scene's arrays (valid until pt_flat_destroy). */
+pt_status pt_flat_desc(const pt_flat *scene, pt_scene_desc *desc);
+pt_status pt_flat_destroy(pt_flat *scene);
+
+/* Reference thin-lens camera (src/core/camera.h:16-43), flattened (flatten_camera). */
+pt_status pt_make_camera(const float lookfrom[3], const float lookat[3], const float vup[3], float vfov_degrees,
+                         float aspect, float aperture, float focus_dist, float time0, float time1, pt_camera *out);
+
+/* Cornell-style box: 10 axis-aligned quads (20 triangles) — floor, back, front, red left,
+ * green right walls, a ceiling of 4 quads around a 0.13 x 0.11 emissive quad of radiance 15 —
+ * plus a diffuse (r = 0.18), a metal (fuzz 0.1) and a dielectric (IOR 1.5) sphere. */
+pt_status pt_workload_cornell(int width, int height, pt_flat **out, pt_camera *camera);
+
+/* Displaced spheres of 2*segments*(rings-1) triangles each (65,536 at 256 x 129) scattered in a
+ * box, with materials drawn per sphere, an optional floor and one emissive quad sized to
+ * `light_fraction` of the total area.  The procedural 1M-triangle scene is
+ * {16, 256, 129, 10, 0.05, 1, 0.005, seed 1}. */
+typedef struct pt_procedural_params {
+    int sphere_count, segments, rings;
+    float box_size;          /* spheres are centered uniformly in [0, box)^3 */
+    float displacement;      /* value-noise amplitude, fraction of the radius */
+    float radius_min, radius_max;
+    int floor;               /* 2-triangle floor below the box */
+    float light_fraction;    /* emissive quad area / total scene area */
+    float light_radiance;
+    float metal_fraction, glass_fraction;
+    uint64_t seed;
+    int random_triangles;    /* extra uniformly placed small triangles (soup) */
+    float soup_edge_min, soup_edge_max;
+} pt_procedural_params;
+void pt_procedural_defaults(pt_procedural_params *params);
+pt_status pt_workload_procedural(const pt_procedural_params *params, int width, int height,
+                                 pt_flat **out, pt_camera *camera);
+
+/* Camera rays of an image, one PCG stream per ray: ray k covers pixel k mod (w*h), jittered like
+ * trace_pixel_sample (src/renderer/transport.h:232-239) with its stream seeded (seed, first+k). */
+pt_status pt_rays_camera(const pt_camera *camera, int width, int height, uint64_t seed, uint64_t first,
+                         size_t count, pt_ray *rays);
+/* Rays leaving random surface points (triangle uniform by index, point uniform by area) with
+ * cosine-distributed directions about a randomly oriented geometric normal.  With shadow_tmax
+ * non-NULL the rays instead aim at a second surface point and shadow_tmax[k] = distance - 0.001,
+ * like the shadow query of src/renderer/transport.h:206-208. */
+pt_status pt_rays_surface(const pt_flat *scene, uint64_t seed, uint64_t first, size_t count,
+                          pt_ray *rays, float *shadow_tmax, int threads);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
