@@ -1,0 +1,314 @@
+"""Benchmark: closest-hit rays per second on the procedural 1M-triangle scene.
+
+Workload (one "step"): one closest-hit pass over 2^25 rays of the 1,048,578-triangle procedural
+scene (16 displaced spheres of 65,536 triangles, a 2-triangle floor, one emissive quad):
+2^24 jittered camera rays of a 960x600 image plus 2^24 cosine-sampled bounce rays leaving their
+closest hits, with tmin 0.001 and tmax FLT_MAX as cuda_query_rays uses.  Inputs (940 MB of rays)
+are larger than L2, so no flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the reference's own CPU traversal (trace_world on host_view, built from
+its sources into oracle/_ref/) on all host threads over a bounded sample of the same rays.
+Under torchrun every rank traces its own replica of the workload (weak scaling, no collective
+on the data path); rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "cuda-path-tracer_b200"))
+import ptb200 as pt  # noqa: E402
+
+METRIC = "Grays/s closest-hit"
+UNIT = "Grays/s"
+WIDTH, HEIGHT = 960, 600
+LOG2_RAYS = 25
+WORKLOAD = "procedural-1M-triangles closest-hit, 2^24 camera + 2^24 bounce rays"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--log2-rays", type=int, default=LOG2_RAYS)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def build_scene():
+    t = time.perf_counter()
+    scene, cam = pt.procedural_scene(WIDTH, HEIGHT)
+    return scene, cam, time.perf_counter() - t
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+        self.dev = device_index
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(device_index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.file, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.file.flush()
+        rows = [r.split(",") for r in Path(self.file.name).read_text().strip().splitlines() if r.strip()]
+        os.unlink(self.file.name)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+            except (ValueError, IndexError):
+                continue
+            for k, name in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].strip().lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def reference_rays(scene, cam, count_each: int, ref):
+    """The first `count_each` camera rays and their bounce rays, built on the host with the
+    reference's own trace_world for the camera hits."""
+    prim = pt.camera_rays(cam, WIDTH, HEIGHT, 1, 0, count_each)
+    res, _ = ref.trace_world(scene, prim)
+    hits = np.zeros(count_each, pt.HIT)
+    m = res["hit"] == 1
+    hits["t"][m] = res["rec"]["t"][m]
+    hits["primitive_id"] = np.where(m, res["rec"]["primitive_id"], -1)
+    hits["primitive_type"] = np.where(m, res["rec"]["primitive_type"], 0)
+    bounce = pt.bounce_rays(scene, prim, hits, 2, 0)
+    return np.concatenate([prim, bounce])
+
+
+def cpu_reference_rate(scene, rays, ref, threads: int):
+    """Reference trace_world over `rays` on `threads` host threads: (rays/s, seconds, stats)."""
+    t = time.perf_counter()
+    _, stats = ref.trace_world(scene, rays, nthreads=threads)
+    dt = time.perf_counter() - t
+    return len(rays) / dt, dt, stats
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    sys.path.insert(0, str(ROOT / "oracle"))
+    from oracle_bind import RefCpu
+    ref = RefCpu()
+    threads = os.cpu_count() or 1
+    scene, cam, _ = build_scene()
+    per = 1 << 16
+    sample = reference_rays(scene, cam, per, ref)
+    for _ in range(args.warmup):
+        cpu_reference_rate(scene, sample, ref, threads)
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        cpu_reference_rate(scene, sample, ref, threads)
+    dt = time.perf_counter() - t
+    value = len(sample) * args.steps / dt / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "sample": f"{len(sample)} rays per step (first 2^16 camera + their bounce rays)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": f"{len(sample)} rays per step, trace_world on host_view"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    scene, cam, t_scene = build_scene()
+    dev = pt.Scene(scene)
+    n_each = 1 << (args.log2_rays - 1)
+    n = 2 * n_each
+    rays = torch.empty(n * 28, dtype=torch.uint8, device="cuda")
+    hits = torch.empty(n * 16, dtype=torch.uint8, device="cuda")
+    pt.camera_rays_device(cam, WIDTH, HEIGHT, 1, 0, n_each, rays)
+    dev.query_device(rays, n_each, hits)
+    dev.bounce_rays_device(rays, hits, n_each, 2, 0, rays[n_each * 28:])
+    torch.cuda.synchronize()
+
+    stream = 0   # legacy default stream: torch's current stream here, and the library's launches
+    launches = []
+    for _ in range(args.warmup):
+        dev.query_device(rays, n, hits, stream=stream)
+    torch.cuda.synchronize()
+    barrier()
+    clocks = Clocks(local)
+    torch.cuda.synchronize()
+    start = torch.cuda.Event(enable_timing=True)
+    stop = torch.cuda.Event(enable_timing=True)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    start.record()
+    for k in range(args.steps):
+        ev[k][0].record()
+        dev.query_device(rays, n, hits, stream=stream)
+        ev[k][1].record()
+    stop.record()
+    torch.cuda.synchronize()
+    clock = clocks.stop()
+    barrier()
+    total_ms = max_over_ranks(start.elapsed_time(stop))
+    per_launch_ms = [a.elapsed_time(b) for a, b in ev]
+    kernel_ms = float(np.mean(per_launch_ms))
+    value = world * n * args.steps / (total_ms / 1e3) / 1e9
+
+    # kernel-own traversal counters (one untimed launch)
+    st = torch.empty(n * 8, dtype=torch.uint8, device="cuda")
+    dev.query_device(rays, n, hits, stats=st)
+    torch.cuda.synchronize()
+    stats = st.view(torch.int32).view(-1, 2).to(torch.float64).mean(0).tolist()
+    hit_rate = float((hits.view(torch.int32).view(-1, 4)[:, 2] != 0).float().mean().item())
+
+    # end to end through the public host-buffer API: pinned rays in, pinned hits out
+    e2e = None
+    if not args.no_e2e:
+        h_rays = torch.empty(n * 28, dtype=torch.uint8, pin_memory=True)
+        h_rays.copy_(rays)
+        h_hits = torch.empty(n * 16, dtype=torch.uint8, pin_memory=True)
+        r_np = h_rays.numpy().view(pt.RAY)
+        lib = pt.library()
+
+        def e2e_step():
+            pt.check(lib.pt_query_rays(dev.handle, h_rays.data_ptr(), n, pt.QUERY_CLOSEST, 0.001, None,
+                                       h_hits.data_ptr(), None))
+        for _ in range(max(1, args.warmup)):
+            e2e_step()
+        torch.cuda.synchronize()
+        barrier()
+        e_steps = max(3, args.steps // 2)
+        t = time.perf_counter()
+        for _ in range(e_steps):
+            e2e_step()
+        torch.cuda.synchronize()
+        e_dt = max_over_ranks(time.perf_counter() - t)
+        e2e = {"value": world * n * e_steps / e_dt / 1e9, "unit": UNIT, "h2d_bytes_per_step": n * 28,
+               "d2h_bytes_per_step": n * 16, "ms_per_step": e_dt / e_steps * 1e3,
+               "api": "pt_query_rays (host buffers, 3-stream chunked pipeline)"}
+        assert h_hits.numpy().view(pt.HIT).size == len(r_np)
+
+    # CPU baseline: the reference's own trace_world on the host cores, bounded sample
+    cpu = None
+    n_box = n_tri = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sys.path.insert(0, str(ROOT / "oracle"))
+        from oracle_bind import RefCpu, REF_CPU_SO
+        if REF_CPU_SO.exists():
+            ref = RefCpu()
+            threads = os.cpu_count() or 1
+            per = 1 << 15
+            sample = reference_rays(scene, cam, per, ref)
+            rate, dt, rstats = cpu_reference_rate(scene, sample, ref, threads)
+            while dt < 3.0 and per < (1 << 20):
+                per *= 4
+                sample = reference_rays(scene, cam, per, ref)
+                rate, dt, rstats = cpu_reference_rate(scene, sample, ref, threads)
+            n_box = float(rstats["boxes"].mean())
+            n_tri = float(rstats["primitives"].mean())
+            cpu = {"value": rate / 1e9, "unit": UNIT, "cores": threads, "kind": "reference",
+                   "sample": f"{len(sample)} rays (first {per} camera rays + their bounce rays), "
+                             f"trace_world on host_view, {dt:.2f} s"}
+
+    peak, peak_kind = measured_peaks()
+    roofline = None
+    if n_box is not None:
+        bytes_per_ray = 32 + 8 + 32 * n_box + 48 * n_tri
+        achieved = bytes_per_ray * n / (kernel_ms / 1e3) / 1e9
+        traffic = None
+        prof = ROOT / "profiles" / "traffic.json"
+        if prof.exists():
+            traffic = json.loads(prof.read_text()).get("query_closest_bytes_per_launch")
+        roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                    "traffic": traffic, "peak_kind": peak_kind,
+                    "algorithmic_bytes_per_ray": bytes_per_ray, "n_box": n_box, "n_tri": n_tri}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "rays_per_step": n, "triangles": int(len(scene.triangles)),
+                   "bvh_nodes": int(len(scene.nodes)), "image": f"{WIDTH}x{HEIGHT}", "l2": "inputs larger than L2 (940 MB rays)",
+                   "parallelism": f"replicas x{world}"},
+        "kernel_ms": kernel_ms, "kernel_stats_per_ray": {"child_boxes": stats[0], "primitives": stats[1]},
+        "hit_rate": hit_rate, "scene_build_s": t_scene,
+        "clocks": clock, "gpu_launches": args.steps,
+        "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    del dev
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

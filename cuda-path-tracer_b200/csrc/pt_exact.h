@@ -184,4 +184,28 @@ PT_HD inline void surface_point(const pt_triangle *tris, uint64_t count, Pcg &r,
     if (r.uniform() < 0.5f) n = -n;
 }
 
+// One bounce ray (pt_rays_bounce / pt_rays_bounce_device): shared by host and device.
+PT_HD inline void bounce_ray(const pt_triangle *tris, uint64_t tri_count, const pt_sphere *spheres, const pt_ray &r,
+                             const pt_hit &h, uint64_t seed, uint64_t index, pt_ray &out) {
+    Pcg g; g.seed(seed, index);
+    f3 p, n;
+    f3 d = mk(r.direction);
+    if (h.primitive_type == PT_TRIANGLE) {
+        const pt_triangle &t = tris[h.primitive_id];
+        p = mk(r.origin) + h.t * d;
+        n = unit(cross(mk(t.v1) - mk(t.v0), mk(t.v2) - mk(t.v0)));
+        if (dot(n, d) > 0) n = -n;
+    } else if (h.primitive_type == PT_SPHERE) {
+        const pt_sphere &sp = spheres[h.primitive_id];
+        p = mk(r.origin) + h.t * d;
+        n = (p - mk(sp.center)) / sp.radius;
+        if (dot(n, d) > 0) n = -n;
+    } else {
+        surface_point(tris, tri_count, g, p, n);
+    }
+    out.origin = pv(p);
+    out.direction = pv(cosine_lift(n, g));
+    out.time = r.time;
+}
+
 } // namespace ptb

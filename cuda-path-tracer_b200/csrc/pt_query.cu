@@ -112,28 +112,8 @@ __global__ void bounce_rays_kernel(DeviceScene s, const pt_ray *primary, const p
                                    uint64_t seed, uint64_t first, uint64_t triangles, pt_ray *out) {
     size_t k = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if(k >= count) return;
-    pt_ray r = primary[k];
-    pt_hit h = hits[k];
-    Pcg g; g.seed(seed, first + k);
-    f3 p, n;
-    f3 d = mk(r.direction);
-    if(h.primitive_type == PT_TRIANGLE) {
-        const pt_triangle &t = s.triangles[h.primitive_id];
-        p = mk(r.origin) + h.t * d;
-        n = unit(cross(mk(t.v1) - mk(t.v0), mk(t.v2) - mk(t.v0)));
-        if(dot(n, d) > 0) n = -n;
-    } else if(h.primitive_type == PT_SPHERE) {
-        const pt_sphere &sp = s.sphere_src[h.primitive_id];
-        p = mk(r.origin) + h.t * d;
-        n = (p - mk(sp.center)) / sp.radius;
-        if(dot(n, d) > 0) n = -n;
-    } else {
-        surface_point(s.triangles, triangles, g, p, n);
-    }
     pt_ray o;
-    o.origin = pv(p);
-    o.direction = pv(cosine_lift(n, g));
-    o.time = r.time;
+    bounce_ray(s.triangles, triangles, s.sphere_src, primary[k], hits[k], seed, first + k, o);
     out[k] = o;
 }
 

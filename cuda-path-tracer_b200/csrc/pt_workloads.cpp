@@ -365,3 +365,29 @@ extern "C" pt_status pt_rays_surface(const pt_flat *scene, uint64_t seed, uint64
         for(auto &th : pool) th.join();
     });
 }
+
+extern "C" pt_status pt_rays_bounce(const pt_flat *scene, const pt_ray *primary, const pt_hit *hits, size_t count,
+                                    uint64_t seed, uint64_t first, pt_ray *rays, int threads) {
+    return guard([&]() {
+        if(!scene || (count && (!primary || !hits || !rays))) throw Error(PT_INVALID_ARGUMENT, "invalid bounce ray arguments");
+        const auto &T = scene->scene.triangles;
+        const auto &S = scene->scene.spheres;
+        if(T.empty()) throw Error(PT_INVALID_ARGUMENT, "bounce rays need triangles");
+        for(size_t k = 0; k < count; k++) {
+            const pt_hit &h = hits[k];
+            if((h.primitive_type == PT_TRIANGLE && (h.primitive_id < 0 || size_t(h.primitive_id) >= T.size())) ||
+               (h.primitive_type == PT_SPHERE && (h.primitive_id < 0 || size_t(h.primitive_id) >= S.size())))
+                throw Error(PT_INVALID_ARGUMENT, "hit refers to a primitive outside the scene");
+        }
+        int nt = threads > 0 ? threads : hardware_threads();
+        if(size_t(nt) > count / 4096 + 1) nt = int(count / 4096 + 1);
+        std::vector<std::thread> pool;
+        for(int t = 0; t < nt; t++) {
+            size_t b = count * size_t(t) / size_t(nt), e = count * size_t(t + 1) / size_t(nt);
+            pool.emplace_back([&, b, e]() {
+                for(size_t k = b; k < e; k++) bounce_ray(T.data(), T.size(), S.data(), primary[k], hits[k], seed, first + k, rays[k]);
+            });
+        }
+        for(auto &th : pool) th.join();
+    });
+}

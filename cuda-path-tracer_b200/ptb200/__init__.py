@@ -125,6 +125,7 @@ def library() -> C.CDLL:
         "pt_workload_procedural": (I, [P, I, I, P, P]),
         "pt_rays_camera": (I, [P, I, I, U64, U64, S, P]),
         "pt_rays_surface": (I, [P, U64, U64, S, P, P, I]),
+        "pt_rays_bounce": (I, [P, P, P, S, U64, U64, P, I]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -290,6 +291,23 @@ def surface_rays(scene: FlatScene, seed: int, first: int, count: int, shadow: bo
         tmax = np.zeros(count, np.float32) if shadow else None
         check(lib.pt_rays_surface(h, seed, first, count, rays.ctypes.data, _ptr(tmax), threads))
         return (rays, tmax) if shadow else rays
+    finally:
+        lib.pt_flat_destroy(h)
+
+
+def bounce_rays(scene: FlatScene, primary: np.ndarray, hits: np.ndarray, seed: int, first: int,
+                threads: int = 0) -> np.ndarray:
+    """Host bounce rays (pt_rays_bounce), bit-identical to Scene.bounce_rays_device."""
+    lib = library()
+    h = C.c_void_p()
+    d = scene.desc()
+    check(lib.pt_flat_from_desc(C.byref(d), C.byref(h)))
+    try:
+        primary = np.ascontiguousarray(primary, RAY)
+        hits = np.ascontiguousarray(hits, HIT)
+        out = np.zeros(len(primary), RAY)
+        check(lib.pt_rays_bounce(h, _ptr(primary), _ptr(hits), len(primary), seed, first, _ptr(out), threads))
+        return out
     finally:
         lib.pt_flat_destroy(h)
 

@@ -1,4 +1,6 @@
-"""ctypes bindings of the CPU oracle and of the reference builds — test infrastructure only.
+"""ctypes bindings of the CPU oracle and of the reference builds — TEST INFRASTRUCTURE ONLY.
+
+Imported only by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline / reference legs.
 
 * ``Oracle``  — oracle/liboracle.so, the C restatement (oracle/pt_oracle.c).
 * ``RefCpu``  — oracle/_ref/libref_cpu.so, the reference's own host code (built from its sources).
@@ -8,13 +10,14 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import sys
 from pathlib import Path
 
 import numpy as np
 
-import ptb200 as pt
-
 ROOT = Path(__file__).resolve().parents[1]
+sys.path.insert(0, str(ROOT / "cuda-path-tracer_b200"))
+import ptb200 as pt  # noqa: E402
 ORACLE_SO = ROOT / "oracle" / "liboracle.so"
 REF_CPU_SO = ROOT / "oracle" / "_ref" / "libref_cpu.so"
 REF_GPU_SO = ROOT / "oracle" / "_ref" / "libref_cuda.so"

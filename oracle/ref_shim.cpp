@@ -48,6 +48,14 @@ flat_scene to_scene(const pt_scene_desc *d) {
     return s;
 }
 
+// scene_view over the caller's arrays (src/renderer/scene_view.h:31-42), no copy.
+scene_view view_of(const pt_scene_desc *d) {
+    scene_view v{reinterpret_cast<const flat_triangle *>(d->triangles), reinterpret_cast<const flat_sphere *>(d->spheres),
+                 reinterpret_cast<const flat_node *>(d->nodes), reinterpret_cast<const flat_material *>(d->materials),
+                 reinterpret_cast<const flat_texture *>(d->textures), d->pixels, d->root, int32_t(d->node_count)};
+    return v;
+}
+
 template <class F> void shard(size_t count, int threads, F fn) {
     if(threads < 1) threads = 1;
     if(size_t(threads) > count) threads = count ? int(count) : 1;
@@ -86,8 +94,7 @@ int ref_scene_lights(const pt_scene_desc *d, pt_light *out, size_t capacity, siz
 // trace_world(host_view(scene), ray, tmin, tmax[i] or FLT_MAX, …) per ray, sharded over threads.
 int ref_trace_world_batch(const pt_scene_desc *d, const pt_ray *rays, size_t count, float tmin,
                           const float *tmax, int brute, pt_trace_result *out, pt_ray_stats *stats, int threads) {
-    auto scene = to_scene(d);
-    scene_view view = host_view(scene);
+    scene_view view = view_of(d);
     auto r = reinterpret_cast<const ray *>(rays);
     shard(count, threads, [&](size_t b, size_t e, int) {
         for(size_t i = b; i < e; i++) {

@@ -19,7 +19,7 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parents[1]
 sys.path.insert(0, str(ROOT / "cuda-path-tracer_b200"))
-sys.path.insert(0, str(ROOT / "tests"))
+sys.path.insert(0, str(ROOT / "oracle"))
 
 import ptb200 as pt  # noqa: E402
 from oracle_bind import RefCpu  # noqa: E402

@@ -1,0 +1,182 @@
+"""GPU parity of the closest-hit / any-hit kernels against the oracle and the reference.
+
+Bar (north star): the same hit primitive as the reference's traversal, exact-distance ties
+resolved to the lowest (type, id), and t within 1e-6 relative.  The kernels reproduce the
+reference's FP32 arithmetic, so these tests demand bit equality of t, which is stricter.
+"""
+from __future__ import annotations
+
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import ptb200 as pt
+from oracle_bind import Oracle, RefGpu, REF_GPU_SO
+
+pytestmark = pytest.mark.gpu
+G = np.load(Path(__file__).parent / "golden" / "reference_golden.npz")
+T_REL = 1e-6   # north-star tolerance on t (the checks below are bitwise, which implies it)
+
+
+def golden_scene(prefix):
+    return pt.FlatScene(G[f"{prefix}_triangles"], G[f"{prefix}_spheres"], G[f"{prefix}_nodes"],
+                        G[f"{prefix}_materials"], G[f"{prefix}_textures"], G[f"{prefix}_pixels"],
+                        int(G[f"{prefix}_root"]), int(G[f"{prefix}_max_depth"]))
+
+
+@pytest.fixture(scope="module")
+def oracle():
+    return Oracle()
+
+
+def assert_hits_equal(got, want):
+    assert got.dtype == pt.HIT and want.dtype == pt.HIT
+    assert np.array_equal(got["primitive_type"], want["primitive_type"])
+    assert np.array_equal(got["primitive_id"], want["primitive_id"])
+    m = want["primitive_type"] != 0
+    assert np.array_equal(got["t"][m].view(np.uint32), want["t"][m].view(np.uint32))
+    rel = np.abs(got["t"][m] - want["t"][m]) / np.maximum(np.abs(want["t"][m]), 1e-30)
+    assert (rel <= T_REL).all()
+    assert not got["error"].any()
+
+
+@pytest.mark.parametrize("brute", [False, True])
+def test_compat_matches_reference_golden(brute):
+    """cuda_query_rays semantics: full 56-byte trace_result, reference tie rule."""
+    s = golden_scene("cornell")
+    got = pt.cuda_query_rays(s, G["cornell_rays"], brute=brute)
+    want = G[f"cornell_result_brute{int(brute)}"]
+    assert got.tobytes() == want.tobytes()
+
+
+def test_compat_reference_pipeline_scene():
+    s = golden_scene("sphere")
+    got = pt.cuda_query_rays(s, G["sphere_rays"])
+    assert got.tobytes() == G["sphere_result"].tobytes()
+
+
+@pytest.mark.parametrize("prefix", ["cornell", "sphere", "light0", "light1"])
+def test_closest_and_any_vs_oracle(oracle, prefix):
+    s = golden_scene(prefix)
+    rays = G["cornell_rays"] if prefix == "cornell" else G["sphere_rays"] if prefix == "sphere" else \
+        pt.camera_rays(G[f"{prefix}_camera"], 19, 13, 5, 0, 2048)
+    dev = pt.Scene(s)
+    assert_hits_equal(dev.query(rays), oracle.query(s, rays))
+    got_any = dev.query(rays, mode=pt.QUERY_ANY)
+    want_any = oracle.query(s, rays, mode=pt.QUERY_ANY)
+    assert np.array_equal(got_any["primitive_type"] != 0, want_any["primitive_id"] >= 0)
+
+
+def test_tmax_and_stats(oracle):
+    s = golden_scene("cornell")
+    rays, tmax = G["cornell_rays"], G["cornell_tmax"]
+    dev = pt.Scene(s)
+    hits, stats = dev.query(rays, tmax=tmax, stats=True)
+    assert_hits_equal(hits, oracle.query(s, rays, tmax=tmax))
+    assert (stats["primitives"] >= (hits["primitive_type"] != 0)).all()
+
+
+def test_exact_tie_lowest_id():
+    """transport_tests' pruning scene (tests/transport_tests.cpp:54-78): two coincident spheres.
+    The reference keeps the later leaf (material 1); the north-star rule keeps the lowest id."""
+    spheres = np.zeros(3, pt.SPHERE)
+    spheres[0] = ((0, 0, 0), 1, 0)
+    spheres[1] = ((0, 0, 0), 1, 1)
+    spheres[2] = ((0, 0, -8), 1, 0)
+    nodes = np.zeros(6, pt.NODE)
+    nodes[0] = ((-1, -1, -9), (1, 1, 1), 0, 1, 4, -1)
+    nodes[1] = ((-1, -1, -1), (1, 1, 1), 0, 2, 3, -1)
+    nodes[2] = ((-1, -1, -1), (1, 1, 1), 2, -1, -1, 0)
+    nodes[3] = ((-1, -1, -1), (1, 1, 1), 2, -1, -1, 1)
+    nodes[4] = ((-1, -1, -9), (1, 1, -7), 0, 5, 5, -1)
+    nodes[5] = ((-1, -1, -9), (1, 1, -7), 2, -1, -1, 2)
+    mats = np.zeros(2, pt.MATERIAL)
+    mats["type"], mats["texture_id"] = 0, 0
+    tex = np.zeros(1, pt.TEXTURE)
+    s = pt.FlatScene(None, spheres, nodes, mats, tex, None, 0, 3)
+    ray = np.zeros(1, pt.RAY)
+    ray[0] = ((0, 0, 3), (0, 0, -1), 0)
+    compat = pt.cuda_query_rays(s, ray)
+    assert compat["hit"][0] == 1 and compat["rec"]["material_id"][0] == 1 and compat["rec"]["t"][0] == 2.0
+    hits = pt.Scene(s).query(ray)
+    assert hits["primitive_id"][0] == 0 and hits["primitive_type"][0] == pt.SPHERE_TYPE and hits["t"][0] == 2.0
+
+
+def test_empty_and_single_primitive_scenes(oracle):
+    empty = pt.FlatScene()
+    rays = G["cornell_rays"][:64]
+    hits = pt.Scene(empty).query(rays)
+    assert (hits["primitive_type"] == 0).all() and (hits["primitive_id"] == -1).all()
+    tri = np.zeros(1, pt.TRIANGLE)
+    tri[0]["v0"], tri[0]["v1"], tri[0]["v2"] = (0, 0, 0), (1, 0, 0), (0, 1, 0)
+    tri[0]["uv1"], tri[0]["uv2"] = (1, 0, 0), (0, 1, 0)
+    mats = np.zeros(1, pt.MATERIAL)
+    tex = np.zeros(1, pt.TEXTURE)
+    one = pt.FlatScene(tri, None, None, mats, tex).build_bvh()
+    assert one.root == 0 and len(one.nodes) == 1
+    r = np.zeros(3, pt.RAY)
+    r[0] = ((0.25, 0.25, 2), (0, 0, -2), 0.4)     # triangle_tests' front hit: t = 1
+    r[1] = ((0.8, 0.8, 1), (0, 0, -1), 0)         # outside
+    r[2] = ((0.5, 0.5, 1), (0, 0, -1), 0)         # on the hypotenuse edge: included
+    got = pt.Scene(one).query(r, tmin=0.0)
+    assert got["t"][0] == 1.0 and got["primitive_id"][0] == 0 and got["primitive_id"][1] == -1 and got["primitive_id"][2] == 0
+    assert_hits_equal(got, oracle.query(one, r, tmin=0.0))
+
+
+def test_brute_device_equals_bvh(oracle):
+    s, cam = pt.cornell_box(64, 40)
+    dev = pt.Scene(s)
+    torch = pytest.importorskip("torch")
+    rays = pt.camera_rays(cam, 64, 40, 9, 0, 8192)
+    d_rays = torch.from_numpy(rays.view(np.uint8).copy()).cuda()
+    a = torch.zeros(len(rays) * 16, dtype=torch.uint8, device="cuda")
+    b = torch.zeros_like(a)
+    dev.query_device(d_rays, len(rays), a)
+    dev.query_device(d_rays, len(rays), b, brute=True)
+    torch.cuda.synchronize()
+    assert torch.equal(a, b)
+
+
+def test_procedural_scene_vs_oracle(oracle):
+    """A 4-sphere, 64k-triangle displaced-sphere scene: camera rays and bounce rays."""
+    torch = pytest.importorskip("torch")
+    s, cam = pt.procedural_scene(96, 60, sphere_count=4, segments=128, rings=65, seed=3)
+    dev = pt.Scene(s)
+    n = 1 << 15
+    prim = torch.zeros(n * 28, dtype=torch.uint8, device="cuda")
+    pt.camera_rays_device(cam, 96, 60, 1, 0, n, prim)
+    hits = torch.zeros(n * 16, dtype=torch.uint8, device="cuda")
+    dev.query_device(prim, n, hits)
+    bounce = torch.zeros_like(prim)
+    dev.bounce_rays_device(prim, hits, n, 2, 0, bounce)
+    hits2 = torch.zeros_like(hits)
+    dev.query_device(bounce, n, hits2)
+    torch.cuda.synchronize()
+    host_prim = prim.cpu().numpy().view(pt.RAY)
+    assert host_prim.tobytes() == pt.camera_rays(cam, 96, 60, 1, 0, n).tobytes()
+    assert_hits_equal(hits.cpu().numpy().view(pt.HIT), oracle.query(s, host_prim))
+    b = bounce.cpu().numpy().view(pt.RAY)
+    assert_hits_equal(hits2.cpu().numpy().view(pt.HIT), oracle.query(s, b))
+    # any-hit shadow rays between surface points
+    sr, tmax = pt.surface_rays(s, 5, 0, 8192, shadow=True)
+    got = dev.query(sr, mode=pt.QUERY_ANY, tmax=tmax)
+    want = oracle.query(s, sr, mode=pt.QUERY_ANY, tmax=tmax)
+    assert np.array_equal(got["primitive_type"] != 0, want["primitive_id"] >= 0)
+
+
+@pytest.mark.skipif(not REF_GPU_SO.exists(), reason="reference CUDA build absent")
+def test_matches_reference_gpu_query():
+    """Our compatibility query and the reference's own cuda_query_rays on the same B200."""
+    s = golden_scene("cornell")
+    want = RefGpu().query(s, G["cornell_rays"])
+    got = pt.cuda_query_rays(s, G["cornell_rays"])
+    assert got.tobytes() == want.tobytes()
+
+
+def test_invalid_scene_is_rejected():
+    s = golden_scene("cornell").copy()
+    s.nodes["left"][s.root] = 9999
+    with pytest.raises(pt.PtError) as e:
+        pt.Scene(s)
+    assert e.value.status == 2
