@@ -28,6 +28,8 @@ struct HostLayout {
     std::vector<SphereRecord> spheres;
     std::vector<int32_t> brute_order;   // leaf slots in flat node-array order
     int32_t empty = 1;
+    float root_lo[3] = {0, 0, 0}, root_hi[3] = {0, 0, 0};
+    int32_t root_leaf = 0;
 };
 HostLayout relayout(const pt_scene_desc &scene);
 

@@ -67,9 +67,13 @@ struct DeviceScene {
     int32_t light_count;
     float light_area;
     int32_t empty;                  // root == -1
+    float root_lo[3], root_hi[3];   // the flat root's own box (tested first by trace_world)
+    int32_t root_leaf;              // flat root is itself a leaf (no branch above it)
 };
 
-// Tie rule for exact-distance hits.
-enum TieRule : int { kTieLowestId = 0, kTieLastLeaf = 1 };
+// Tie rule for exact-distance hits: the lowest (type, id) (north-star rule), the leaf the
+// reference's depth-first walk reaches last (trace_world, src/renderer/transport.h:76-79), or
+// the last leaf in node-array order (its brute-force scan, transport.h:48-60).
+enum TieRule : int { kTieLowestId = 0, kTieLastLeaf = 1, kTieLastNode = 2 };
 
 } // namespace ptb

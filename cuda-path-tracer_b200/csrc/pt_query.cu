@@ -79,7 +79,7 @@ __global__ void __launch_bounds__(kQueryBlock) compat_kernel(DeviceScene s, cons
     HitInfo h;
     uint32_t boxes = 0, prims = 0;
     int error = 0;
-    bool hit = brute ? traverse_brute<false>(s, order, leaves, r, 0.001f, FLT_MAX, kTieLastLeaf, h, prims)
+    bool hit = brute ? traverse_brute<false>(s, order, leaves, r, 0.001f, FLT_MAX, kTieLastNode, h, prims)
                      : traverse<false>(s, r, 0.001f, FLT_MAX, kTieLastLeaf, h, boxes, prims, error);
     pt_trace_result res;
     res.rec.t = 0; res.rec.u = 0; res.rec.v = 0;
@@ -211,6 +211,8 @@ pt_status pt_scene_create(const pt_scene_desc *desc, pt_scene **out) {
             v.light_count = int32_t(lights.size());
             v.light_area = area;
             v.empty = layout.empty;
+            for(int a = 0; a < 3; a++) { v.root_lo[a] = layout.root_lo[a]; v.root_hi[a] = layout.root_hi[a]; }
+            v.root_leaf = layout.root_leaf;
         } catch(...) { delete sc; throw; }
         *out = sc;
     });

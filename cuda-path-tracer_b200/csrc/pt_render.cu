@@ -1,0 +1,536 @@
+// pt_render.cu — wavefront MIS path tracer (sm_100a, built with --fmad=false).
+//
+// Replaces class cuda_renderer and its render_pixels megakernel (src/cuda/cuda_renderer.cu:64-240).
+// The reference runs trace_pixel_sample's whole bounce loop in one thread per pixel.  Here a
+// path's bounce loop is cut into three kernels that run over queues of live paths:
+//   extend : closest hit of every queued path's ray,
+//   shade  : the rest of one trace_color iteration (emission with MIS weight, next-event
+//            estimation that emits a shadow ray, cosine or material scatter), and, when a
+//            sample ends, its radiance added to the pixel sum and the pixel's next camera ray,
+//   shadow : any-hit of the shadow rays; an unoccluded one adds its precomputed contribution.
+// Exactly one path per pixel is in flight, so every pixel's PCG stream is consumed in the
+// reference's order and every float is summed in the reference's order: with the same
+// arithmetic (--fmad=false, the same CUDA math functions) the sums, RNG states and ray count
+// equal the reference renderer's.
+#include <cfloat>
+#include <cstring>
+#include <vector>
+#include "pt_api_common.h"
+#include "pt_device.h"
+#include "pt_shade.h"
+
+using namespace ptb;
+
+namespace ptb {
+
+struct alignas(16) PathState {
+    float ox, oy, oz, time;
+    float dx, dy, dz, prev_pdf;
+    float tr, tg, tb; int32_t depth;
+    float rr, rg, rb; int32_t samples_left;
+};
+struct alignas(16) PathHit { float t, u, v; int32_t slot; };
+struct alignas(16) ShadowRay {
+    float ox, oy, oz, tmax;
+    float dx, dy, dz, time;
+    float cr, cg, cb; int32_t pixel;
+};
+static_assert(sizeof(PathState) == 64 && sizeof(PathHit) == 16 && sizeof(ShadowRay) == 48, "path records");
+
+struct RenderParams {
+    pt_camera camera;
+    int width, height, max_depth, debug, mis, brute;
+    int32_t leaves;
+    const int32_t *brute_order;
+};
+
+struct RenderBuffers {
+    PathState *paths;
+    PathHit *hits;
+    uint2 *stats;           // per-path box/primitive counts (bvh / intersections views)
+    ShadowRay *shadows;
+    int32_t *queue[2];
+    int32_t *shadow_queue;
+    int32_t *counters;      // [0],[1]: path queues; [2]: shadow queue
+    unsigned long long *rays;
+    int32_t *error;
+    float *sums;
+    Pcg *rng;
+};
+
+__device__ inline unsigned lane_id() { return threadIdx.x & 31; }
+
+// Warp-aggregated append: one atomicAdd per warp.
+__device__ inline void push(bool take, int32_t value, int32_t *queue, int32_t *counter) {
+    unsigned m = __ballot_sync(0xffffffffu, take);
+    if (!m) return;
+    int leader = __ffs(m) - 1;
+    int base = 0;
+    if ((int)lane_id() == leader) base = atomicAdd(counter, __popc(m));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (take) queue[base + __popc(m & ((1u << lane_id()) - 1u))] = value;
+}
+
+// trace_pixel_sample's camera step (src/renderer/transport.h:232-239)
+__device__ inline void camera_path(const RenderParams &p, int32_t pixel, Pcg &rng, PathState &s) {
+    int x = pixel % p.width, y = pixel / p.width;
+    float u = (x + rng.uniform()) / float(p.width);
+    float v = (y + rng.uniform()) / float(p.height);
+    pt_ray r;
+    camera_ray(p.camera, u, v, rng, r);
+    s.ox = r.origin.x; s.oy = r.origin.y; s.oz = r.origin.z; s.time = r.time;
+    s.dx = r.direction.x; s.dy = r.direction.y; s.dz = r.direction.z; s.prev_pdf = 0;
+    s.tr = 1; s.tg = 1; s.tb = 1; s.depth = 0;
+    s.rr = 0; s.rg = 0; s.rb = 0;
+}
+
+// initialize_pixels (src/cuda/cuda_renderer.cu:64-68)
+__global__ void init_pixels(float *sums, Pcg *rng, int32_t count, uint64_t seed) {
+    int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    sums[3 * i] = 0; sums[3 * i + 1] = 0; sums[3 * i + 2] = 0;
+    Pcg r; r.seed(seed, uint64_t(i));
+    rng[i] = r;
+}
+
+// First camera ray of every pixel; queue 0 = all pixels in order.
+__global__ void start_samples(RenderParams p, RenderBuffers b, int32_t count, int samples) {
+    int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) { b.counters[0] = count; b.counters[1] = 0; b.counters[2] = 0; }
+    if (i >= count) return;
+    Pcg rng = b.rng[i];
+    PathState s;
+    camera_path(p, i, rng, s);
+    s.samples_left = samples;
+    b.rng[i] = rng;
+    b.paths[i] = s;
+    b.queue[0][i] = i;
+}
+
+__device__ inline pt_ray path_ray(const PathState &s) {
+    pt_ray r;
+    r.origin = pt_vec3{s.ox, s.oy, s.oz};
+    r.direction = pt_vec3{s.dx, s.dy, s.dz};
+    r.time = s.time;
+    return r;
+}
+
+// extend: closest hit of each queued path (trace_color's trace_world, transport.h:177-178)
+__global__ void extend_kernel(DeviceScene scene, RenderParams p, RenderBuffers b, int parity) {
+    const int32_t n = b.counters[parity];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        atomicAdd(b.rays, (unsigned long long)n);
+        b.counters[parity ^ 1] = 0;      // the next queue fills during shade
+        b.counters[2] = 0;
+    }
+    const bool reference_order = p.debug == PT_DEBUG_BVH || p.debug == PT_DEBUG_INTERSECTIONS;
+    for (int32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        int32_t i = b.queue[parity][k];
+        PathState s = b.paths[i];
+        pt_ray r = path_ray(s);
+        HitInfo h;
+        uint32_t boxes = 0, prims = 0;
+        int error = 0;
+        bool hit;
+        if (p.brute) hit = traverse_brute<false>(scene, p.brute_order, p.leaves, r, 0.001f, FLT_MAX, kTieLastNode, h, prims);
+        else if (reference_order) hit = traverse_reference(scene, r, 0.001f, FLT_MAX, kTieLastLeaf, h, boxes, prims, error);
+        else hit = traverse<false>(scene, r, 0.001f, FLT_MAX, kTieLastLeaf, h, boxes, prims, error);
+        if (error) *b.error = 1;
+        PathHit out;
+        out.t = h.t; out.u = h.u; out.v = h.v; out.slot = (hit && !error) ? h.slot : (error ? -2 : -1);
+        b.hits[i] = out;
+        if (reference_order) b.stats[i] = make_uint2(boxes, prims);
+    }
+}
+
+// shade: the rest of one trace_color iteration (transport.h:179-228)
+__global__ void shade_kernel(DeviceScene scene, RenderParams p, RenderBuffers b, int parity) {
+    const int32_t n = b.counters[parity];
+    const int32_t *in = b.queue[parity];
+    int32_t *out = b.queue[parity ^ 1];
+    for (int32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        int32_t k = base + threadIdx.x;
+        bool valid = k < n;
+        bool live = false, shadow = false;
+        int32_t i = valid ? in[k] : 0;
+        ShadowRay sr;
+        if (valid) {
+            PathState s = b.paths[i];
+            PathHit h = b.hits[i];
+            Pcg rng = b.rng[i];
+            f3 radiance = mk(s.rr, s.rg, s.rb);
+            f3 throughput = mk(s.tr, s.tg, s.tb);
+            bool finished = false;
+            if (p.debug == PT_DEBUG_BVH || p.debug == PT_DEBUG_INTERSECTIONS) {
+                uint2 st = b.stats[i];
+                float cost = log2f(1.0f + float(p.debug == PT_DEBUG_BVH ? st.x : st.y)) / 10.0f;
+                cost = fminf(1, cost);
+                radiance = mk(cost, cost * cost, 1 - cost);
+                finished = true;
+            } else if (h.slot < 0) {
+                finished = true;                       // miss, or a traversal error
+            } else {
+                pt_ray r = path_ray(s);
+                HitInfo hi; hi.t = h.t; hi.u = h.u; hi.v = h.v; hi.slot = h.slot;
+                pt_flat_hit rec;
+                finalize_hit(scene, r, hi, rec);
+                if (p.debug == PT_DEBUG_NORMALS) { radiance = 0.5f * (mk(rec.normal) + mk(1, 1, 1)); finished = true; }
+                else if (p.debug == PT_DEBUG_TRIANGLE) {
+                    radiance = rec.primitive_type == PT_TRIANGLE ? id_color(rec.primitive_id) : mk(0.3f, 0.3f, 0.3f);
+                    finished = true;
+                } else if (p.debug == PT_DEBUG_MATERIAL) { radiance = id_color(rec.material_id); finished = true; }
+                else {
+                    const pt_material mat = scene.materials[rec.material_id];
+                    f3 in_dir = mk(s.dx, s.dy, s.dz);
+                    f3 pos = mk(rec.p), normal = mk(rec.normal);
+                    if (mat.type == PT_LIGHT) {
+                        float weight = s.prev_pdf > 0 ? mis_weight(s.prev_pdf, hit_light_pdf(scene, mk(s.ox, s.oy, s.oz), rec)) : 1;
+                        radiance = radiance + weight * throughput * trace_texture(scene, mat.texture_id, rec.u, rec.v);
+                        finished = true;
+                    } else if (s.depth == p.max_depth) {
+                        finished = true;
+                    } else if (p.mis && mat.type == PT_DIFFUSE) {
+                        f3 attenuation = trace_texture(scene, mat.texture_id, rec.u, rec.v);
+                        if (scene.light_count) {
+                            LightSample light = sample_light(scene, rng);
+                            f3 delta = light.point - pos;
+                            float distance = length(delta);
+                            if (distance > 0.002f && finite(distance)) {
+                                f3 direction = delta / distance;
+                                float cosine = fmaxf(0, dot(normal, direction));
+                                float pdf = light_direction_pdf(scene.light_area, pos, light.point, light.normal);
+                                if (cosine > 0 && pdf > 0) {
+                                    const pt_material &emitter = scene.materials[light.material];
+                                    f3 emission = trace_texture(scene, emitter.texture_id, light.u, light.v);
+                                    float bsdf_pdf = cosine / float(M_PI);
+                                    f3 c = throughput * attenuation * emission * (bsdf_pdf * mis_weight(pdf, bsdf_pdf) / pdf);
+                                    sr.ox = pos.x; sr.oy = pos.y; sr.oz = pos.z; sr.tmax = distance - 0.001f;
+                                    sr.dx = direction.x; sr.dy = direction.y; sr.dz = direction.z; sr.time = s.time;
+                                    sr.cr = c.x; sr.cg = c.y; sr.cb = c.z; sr.pixel = i;
+                                    shadow = true;
+                                }
+                            }
+                        }
+                        f3 direction = cosine_direction(normal, rng);
+                        s.prev_pdf = fmaxf(0, dot(normal, direction)) / float(M_PI);
+                        throughput = throughput * attenuation;
+                        s.ox = pos.x; s.oy = pos.y; s.oz = pos.z;
+                        s.dx = direction.x; s.dy = direction.y; s.dz = direction.z;
+                        s.depth++;
+                    } else {
+                        s.prev_pdf = 0;
+                        f3 attenuation, dir;
+                        if (!trace_scatter(scene, mat, in_dir, rec, rng, attenuation, dir)) finished = true;
+                        else {
+                            throughput = throughput * attenuation;
+                            s.ox = pos.x; s.oy = pos.y; s.oz = pos.z;
+                            s.dx = dir.x; s.dy = dir.y; s.dz = dir.z;
+                            s.depth++;
+                        }
+                    }
+                }
+            }
+            if (finished) {
+                // accumulated += trace_pixel_sample(...) (src/cuda/cuda_renderer.cu:81)
+                float *sum = b.sums + 3 * size_t(i);
+                sum[0] = sum[0] + radiance.x; sum[1] = sum[1] + radiance.y; sum[2] = sum[2] + radiance.z;
+                s.samples_left--;
+                if (s.samples_left > 0) {
+                    int left = s.samples_left;
+                    camera_path(p, i, rng, s);
+                    s.samples_left = left;
+                    live = true;
+                }
+            } else {
+                s.tr = throughput.x; s.tg = throughput.y; s.tb = throughput.z;
+                s.rr = radiance.x; s.rg = radiance.y; s.rb = radiance.z;
+                live = true;
+            }
+            b.paths[i] = s;
+            b.rng[i] = rng;
+            if (shadow) b.shadows[i] = sr;
+        }
+        push(live, i, out, &b.counters[parity ^ 1]);
+        push(shadow, i, b.shadow_queue, &b.counters[2]);
+    }
+}
+
+// shadow: any-hit of the NEE rays (transport.h:206-214); unoccluded ones add their contribution
+__global__ void shadow_kernel(DeviceScene scene, RenderParams p, RenderBuffers b) {
+    const int32_t n = b.counters[2];
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(b.rays, (unsigned long long)n);
+    for (int32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        int32_t i = b.shadow_queue[k];
+        ShadowRay sr = b.shadows[i];
+        pt_ray r;
+        r.origin = pt_vec3{sr.ox, sr.oy, sr.oz};
+        r.direction = pt_vec3{sr.dx, sr.dy, sr.dz};
+        r.time = sr.time;
+        HitInfo h;
+        uint32_t boxes = 0, prims = 0;
+        int error = 0;
+        bool blocked = p.brute ? traverse_brute<true>(scene, p.brute_order, p.leaves, r, 0.001f, sr.tmax, kTieLastNode, h, prims)
+                               : traverse<true>(scene, r, 0.001f, sr.tmax, kTieLastLeaf, h, boxes, prims, error);
+        if (error) { *b.error = 1; continue; }
+        if (!blocked) {
+            PathState &s = b.paths[i];
+            s.rr = s.rr + sr.cr; s.rg = s.rg + sr.cg; s.rb = s.rb + sr.cb;
+        }
+    }
+}
+
+// pack_pixels (src/cuda/cuda_renderer.cu:99-109)
+__global__ void pack_pixels(const float *sum, unsigned char *rgba, size_t count, int samples) {
+    size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    f3 color = samples ? mk(sum[3 * i], sum[3 * i + 1], sum[3 * i + 2]) / float(samples) : mk(0, 0, 0);
+    for (int channel = 0; channel < 3; channel++) {
+        float value = comp(color, channel);
+        float gamma = value > 0 && value < 1 ? sqrtf(value) : 0;
+        rgba[4 * i + channel] = !(value > 0) ? 0 : value >= 1 ? 255 : int(255.99 * gamma);
+    }
+    rgba[4 * i + 3] = 255;
+}
+
+int occupancy_grid(const void *kernel, int block) {
+    int per_sm = 0;
+    PT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0));
+    return device_sm_count() * (per_sm > 0 ? per_sm : 1);
+}
+
+} // namespace ptb
+
+struct pt_renderer {
+    const pt_scene *scene = nullptr;
+    RenderParams params{};
+    uint64_t seed = 0;
+    int32_t pixels = 0;
+    int samples = 0;
+    float milliseconds = 0;
+    uint64_t rays = 0;
+    int block = 256;
+    int grid_extend = 0, grid_shade = 0, grid_shadow = 0;
+    DeviceBuffer paths, hits, stats, shadows, queue0, queue1, shadow_queue, counters, ray_total, error, sums, rng, rgba;
+    RenderBuffers buf{};
+    cudaStream_t stream = nullptr;
+    Event start, stop;
+    int32_t *host_counters = nullptr;   // pinned, one slot per in-flight iteration
+    Event iteration_events[8];
+    ~pt_renderer() {
+        if (host_counters) cudaFreeHost(host_counters);
+        if (stream) cudaStreamDestroy(stream);
+    }
+    void grids() {
+        grid_extend = occupancy_grid((const void *)extend_kernel, block);
+        grid_shade = occupancy_grid((const void *)shade_kernel, block);
+        grid_shadow = occupancy_grid((const void *)shadow_kernel, block);
+    }
+};
+
+namespace {
+void validate_camera(const pt_camera &c) {
+    // validate_render_camera, src/renderer/render_validation.h:16-22
+    for (const pt_vec3 &v : {c.origin, c.lower_left_corner, c.horizontal, c.vertical, c.u, c.v})
+        if (!std::isfinite(v.x) || !std::isfinite(v.y) || !std::isfinite(v.z))
+            throw Error(PT_INVALID_ARGUMENT, "camera contains nonfinite values");
+    if (!std::isfinite(c.lens_radius) || c.lens_radius < 0 || !std::isfinite(c.time0) || !std::isfinite(c.time1) || c.time1 < c.time0)
+        throw Error(PT_INVALID_ARGUMENT, "invalid camera lens/shutter");
+}
+constexpr int kIterationRing = 8;   // == size of pt_renderer::iteration_events
+} // namespace
+
+extern "C" {
+
+pt_status pt_renderer_create(const pt_scene *scene, const pt_camera *camera, int width, int height, uint64_t seed,
+                             uint32_t flags, int debug_mode, int max_depth, pt_renderer **out) {
+    return guard([&]() {
+        if (!scene || !camera || !out) throw Error(PT_INVALID_ARGUMENT, "null argument");
+        *out = nullptr;
+        // checked_pixel_count and validate_render_mode (src/renderer/render_validation.h:7-15)
+        if (width <= 0 || height <= 0 || uint64_t(width) * uint64_t(height) > uint64_t(INT32_MAX))
+            throw Error(PT_INVALID_ARGUMENT, "image dimensions exceed supported pixel count");
+        if (debug_mode < PT_DEBUG_SHADED || debug_mode > PT_DEBUG_INTERSECTIONS) throw Error(PT_INVALID_ARGUMENT, "invalid render debug mode");
+        if (max_depth < 0 || max_depth > 100000) throw Error(PT_INVALID_ARGUMENT, "invalid bounce limit");
+        validate_camera(*camera);
+        require_device();
+        auto r = new pt_renderer;
+        try {
+            size_t n = size_t(width) * size_t(height);
+            r->scene = scene;
+            r->seed = seed;
+            r->pixels = int32_t(n);
+            RenderParams &p = r->params;
+            p.camera = *camera; p.width = width; p.height = height; p.max_depth = max_depth;
+            p.debug = debug_mode; p.mis = (flags & PT_RENDER_MIS) ? 1 : 0; p.brute = (flags & PT_RENDER_BRUTE) ? 1 : 0;
+            p.leaves = scene->leaf_count; p.brute_order = scene->brute_order.get<int32_t>();
+            r->paths.resize(n * sizeof(PathState));
+            r->hits.resize(n * sizeof(PathHit));
+            if (debug_mode == PT_DEBUG_BVH || debug_mode == PT_DEBUG_INTERSECTIONS) r->stats.resize(n * sizeof(uint2));
+            r->shadows.resize(n * sizeof(ShadowRay));
+            r->queue0.resize(n * sizeof(int32_t));
+            r->queue1.resize(n * sizeof(int32_t));
+            r->shadow_queue.resize(n * sizeof(int32_t));
+            r->counters.resize(4 * sizeof(int32_t));
+            r->ray_total.resize(sizeof(unsigned long long));
+            r->error.resize(sizeof(int32_t));
+            r->sums.resize(n * 3 * sizeof(float));
+            r->rng.resize(n * sizeof(Pcg));
+            RenderBuffers &b = r->buf;
+            b.paths = r->paths.get<PathState>(); b.hits = r->hits.get<PathHit>(); b.stats = r->stats.get<uint2>();
+            b.shadows = r->shadows.get<ShadowRay>();
+            b.queue[0] = r->queue0.get<int32_t>(); b.queue[1] = r->queue1.get<int32_t>();
+            b.shadow_queue = r->shadow_queue.get<int32_t>(); b.counters = r->counters.get<int32_t>();
+            b.rays = r->ray_total.get<unsigned long long>(); b.error = r->error.get<int32_t>();
+            b.sums = r->sums.get<float>(); b.rng = r->rng.get<Pcg>();
+            PT_CUDA(cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking));
+            PT_CUDA(cudaMallocHost(&r->host_counters, kIterationRing * sizeof(int32_t)));
+            r->grids();
+        } catch (...) { delete r; throw; }
+        *out = r;
+        pt_status st = pt_reset(r, camera);
+        if (st != PT_OK) { delete r; *out = nullptr; throw Error(st, pt_last_error()); }
+    });
+}
+
+pt_status pt_renderer_destroy(pt_renderer *r) { delete r; return PT_OK; }
+
+// reset(camera) (src/cuda/cuda_renderer.cu:186-194)
+pt_status pt_reset(pt_renderer *r, const pt_camera *camera) {
+    return guard([&]() {
+        if (!r || !camera) throw Error(PT_INVALID_ARGUMENT, "null argument");
+        validate_camera(*camera);
+        PT_CUDA(cudaMemsetAsync(r->buf.error, 0, sizeof(int32_t), r->stream));
+        init_pixels<<<(r->pixels + 255) / 256, 256, 0, r->stream>>>(r->buf.sums, r->buf.rng, r->pixels, r->seed);
+        PT_CUDA(cudaGetLastError());
+        PT_CUDA(cudaStreamSynchronize(r->stream));
+        r->params.camera = *camera;
+        r->samples = 0; r->milliseconds = 0; r->rays = 0;
+    });
+}
+
+// add_samples(count) (src/cuda/cuda_renderer.cu:196-213)
+pt_status pt_add_samples(pt_renderer *r, int count) {
+    return guard([&]() {
+        if (!r) throw Error(PT_INVALID_ARGUMENT, "null renderer");
+        if (count <= 0 || count > INT32_MAX - r->samples) throw Error(PT_INVALID_ARGUMENT, "invalid accumulated sample count");
+        const DeviceScene &scene = r->scene->view;
+        cudaStream_t st = r->stream;
+        PT_CUDA(cudaMemsetAsync(r->buf.rays, 0, sizeof(unsigned long long), st));
+        PT_CUDA(cudaEventRecord(r->start.get(), st));
+        start_samples<<<(r->pixels + 255) / 256, 256, 0, st>>>(r->params, r->buf, r->pixels, count);
+        PT_CUDA(cudaGetLastError());
+        // Every pixel needs at most count * (max_depth + 1) extends; the loop ends earlier when
+        // the queue is empty.  The queue length is read back with a lag of a few iterations.
+        const int64_t max_iterations = int64_t(count) * (int64_t(r->params.max_depth) + 1) + 1;
+        int parity = 0;
+        int64_t issued = 0, checked = 0;
+        bool done = false;
+        while (!done && issued < max_iterations) {
+            extend_kernel<<<r->grid_extend, r->block, 0, st>>>(scene, r->params, r->buf, parity);
+            shade_kernel<<<r->grid_shade, r->block, 0, st>>>(scene, r->params, r->buf, parity);
+            shadow_kernel<<<r->grid_shadow, r->block, 0, st>>>(scene, r->params, r->buf);
+            PT_CUDA(cudaGetLastError());
+            parity ^= 1;
+            int slot = int(issued % kIterationRing);
+            PT_CUDA(cudaMemcpyAsync(&r->host_counters[slot], &r->buf.counters[parity], sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+            PT_CUDA(cudaEventRecord(r->iteration_events[slot].get(), st));
+            issued++;
+            // keep at most kIterationRing/2 iterations ahead of the last one inspected
+            while (checked < issued && (issued - checked >= kIterationRing / 2 ||
+                                        cudaEventQuery(r->iteration_events[int(checked % kIterationRing)].get()) == cudaSuccess)) {
+                PT_CUDA(cudaEventSynchronize(r->iteration_events[int(checked % kIterationRing)].get()));
+                if (r->host_counters[int(checked % kIterationRing)] == 0) { done = true; break; }
+                checked++;
+            }
+        }
+        while (!done && checked < issued) {   // iterations issued but not yet inspected
+            PT_CUDA(cudaEventSynchronize(r->iteration_events[int(checked % kIterationRing)].get()));
+            if (r->host_counters[int(checked % kIterationRing)] == 0) done = true;
+            checked++;
+        }
+        PT_CUDA(cudaEventRecord(r->stop.get(), st));
+        PT_CUDA(cudaEventSynchronize(r->stop.get()));
+        int32_t error = 0;
+        unsigned long long total = 0;
+        PT_CUDA(cudaMemcpy(&error, r->buf.error, sizeof error, cudaMemcpyDeviceToHost));
+        if (error) throw Error(PT_STACK_OVERFLOW, "CUDA traversal stack overflow");
+        if (!done) throw Error(PT_TIMEOUT, "wavefront did not drain within its iteration bound");
+        float ms = 0;
+        PT_CUDA(cudaEventElapsedTime(&ms, r->start.get(), r->stop.get()));
+        PT_CUDA(cudaMemcpy(&total, r->buf.rays, sizeof total, cudaMemcpyDeviceToHost));
+        r->milliseconds += ms;
+        r->samples += count;
+        r->rays += total;
+    });
+}
+
+// set_block_shape (src/cuda/cuda_renderer.cu:215-228): the accepted shapes, as block sizes.
+pt_status pt_set_block_shape(pt_renderer *r, int width, int height) {
+    return guard([&]() {
+        if (!r) throw Error(PT_INVALID_ARGUMENT, "null renderer");
+        if (!((width == 8 && height == 8) || (width == 16 && height == 8) || (width == 16 && height == 16) || (width == 32 && height == 8)))
+            throw Error(PT_INVALID_ARGUMENT, "CUDA block must be 8x8, 16x8, 16x16 or 32x8");
+        r->block = width * height;
+        r->grids();
+    });
+}
+
+pt_status pt_get_sums(const pt_renderer *r, float *rgb, size_t floats) {
+    return guard([&]() {
+        if (!r || !rgb || floats < size_t(r->pixels) * 3) throw Error(PT_INVALID_ARGUMENT, "sum buffer too small");
+        PT_CUDA(cudaMemcpy(rgb, r->buf.sums, size_t(r->pixels) * 3 * sizeof(float), cudaMemcpyDeviceToHost));
+    });
+}
+
+// image(): sums scaled by vec3::operator/= (reciprocal taken in double), on the host like the reference
+pt_status pt_get_image(const pt_renderer *r, float *rgb, size_t floats) {
+    return guard([&]() {
+        pt_status st = pt_get_sums(r, rgb, floats);
+        if (st != PT_OK) throw Error(st, pt_last_error());
+        if (!r->samples) return;
+        float k = (float)(1.0 / (double)float(r->samples));
+        for (size_t i = 0; i < size_t(r->pixels) * 3; i++) rgb[i] *= k;
+    });
+}
+
+pt_status pt_get_rng(const pt_renderer *r, uint64_t *words, size_t count) {
+    return guard([&]() {
+        if (!r || !words || count < size_t(r->pixels) * 2) throw Error(PT_INVALID_ARGUMENT, "rng buffer too small");
+        PT_CUDA(cudaMemcpy(words, r->buf.rng, size_t(r->pixels) * sizeof(Pcg), cudaMemcpyDeviceToHost));
+    });
+}
+
+pt_status pt_write_rgba(const pt_renderer *r, unsigned char *device_pixels, size_t bytes) {
+    return guard([&]() {
+        if (!r) throw Error(PT_INVALID_ARGUMENT, "null renderer");
+        size_t count = size_t(r->pixels);
+        if (!device_pixels || bytes < 4 * count) throw Error(PT_INVALID_ARGUMENT, "CUDA RGBA destination is too small");
+        pack_pixels<<<unsigned((count + 255) / 256), 256, 0, r->stream>>>(r->buf.sums, device_pixels, count, r->samples);
+        PT_CUDA(cudaGetLastError());
+        PT_CUDA(cudaStreamSynchronize(r->stream));
+    });
+}
+
+pt_status pt_rgba_image(const pt_renderer *cr, unsigned char *host_pixels, size_t bytes) {
+    return guard([&]() {
+        pt_renderer *r = const_cast<pt_renderer *>(cr);
+        if (!r) throw Error(PT_INVALID_ARGUMENT, "null renderer");
+        size_t count = size_t(r->pixels);
+        if (!host_pixels || bytes < 4 * count) throw Error(PT_INVALID_ARGUMENT, "RGBA destination is too small");
+        r->rgba.reserve(4 * count);
+        pt_status st = pt_write_rgba(r, r->rgba.get<unsigned char>(), 4 * count);
+        if (st != PT_OK) throw Error(st, pt_last_error());
+        PT_CUDA(cudaMemcpy(host_pixels, r->rgba.get(), 4 * count, cudaMemcpyDeviceToHost));
+    });
+}
+
+pt_status pt_stats(const pt_renderer *r, int *samples, float *kernel_ms, uint64_t *rays) {
+    return guard([&]() {
+        if (!r) throw Error(PT_INVALID_ARGUMENT, "null renderer");
+        if (samples) *samples = r->samples;
+        if (kernel_ms) *kernel_ms = r->milliseconds;
+        if (rays) *rays = r->rays;
+    });
+}
+
+} // extern "C"

@@ -171,6 +171,10 @@ HostLayout relayout(const pt_scene_desc &s) {
     if(s.root < 0) { out.empty = 1; return out; }
     out.empty = 0;
     const pt_node *nodes = s.nodes;
+    const pt_node &rootn = nodes[s.root];
+    out.root_lo[0] = rootn.minimum.x; out.root_lo[1] = rootn.minimum.y; out.root_lo[2] = rootn.minimum.z;
+    out.root_hi[0] = rootn.maximum.x; out.root_hi[1] = rootn.maximum.y; out.root_hi[2] = rootn.maximum.z;
+    out.root_leaf = rootn.type != PT_BRANCH;
     std::vector<int32_t> inner(s.node_count, -1), slot(s.node_count, -1);
     std::vector<int32_t> tri_leaves, sphere_leaves;   // flat node ids per slot
     // Pass 1: number branches and leaves in preorder (left before right, as trace_world pops).

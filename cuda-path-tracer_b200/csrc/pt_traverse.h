@@ -28,7 +28,10 @@ struct HitInfo {
 #define PT_LDGI4(p) __ldg(reinterpret_cast<const int4 *>(p))
 #endif
 
+// Smaller key wins an exact-distance tie.  Slots are numbered in the reference walk's
+// first-visit order, so the last leaf it reaches has the largest slot.
 PT_HD inline long long tie_key(const DeviceScene &s, int32_t slot, int tie) {
+    if (tie == kTieLastLeaf) return -(long long)slot;
     if (slot < s.tri_slots) {
         const TriRecord &t = s.tris[slot];
         return tie == kTieLowestId ? ((1ll << 32) | (uint32_t)t.id) : -(long long)t.node;
@@ -145,6 +148,71 @@ PT_HD inline bool traverse(const DeviceScene &s, const pt_ray &r, float tmin, fl
         } else {
             if (sp == 0) break;
             node = stack[--sp];
+        }
+    }
+    return found;
+}
+
+// trace_world in the reference's own visiting order (src/renderer/transport.h:61-84): a
+// branch's box is tested when it is popped, its right child pushed below its left, leaves
+// tested without a box test.  Same answer as traverse<>; used where the reference's per-ray
+// counts matter (the bvh / intersections debug views count boxes and primitives like its
+// trace_stats).  Stack entries are (parent node << 1 | side) so the popped child's box is
+// read from its parent.
+PT_HD inline bool traverse_reference(const DeviceScene &s, const pt_ray &r, float tmin, float tmax, int tie,
+                                     HitInfo &hit, uint32_t &boxes, uint32_t &prims, int &error) {
+    hit.slot = -1; hit.t = 0; hit.u = 0; hit.v = 0;
+    if (s.empty || s.node_count == 0) return false;
+    RayBox rb = ray_box(r);
+    float dl = length(mk(r.direction));
+    bool found = false;
+    float closest = tmax;
+    long long best_key = 0;
+    if (s.root_leaf) {
+        BvhNode n;
+        load_node(s, 0, n);
+        test_leaf<false>(s, ~n.child0, r, dl, tmin, tmax, tie, found, closest, best_key, hit, prims);
+        return found;
+    }
+    // the root branch: its own box first
+    {
+        boxes++;
+        float e;
+        if (!box_hit(rb, s.root_lo[0], s.root_hi[0], s.root_lo[1], s.root_hi[1], s.root_lo[2], s.root_hi[2], tmin, tmax, e))
+            return false;
+    }
+    int32_t stack[kStackCapacity];
+    int sp = 0;
+    // children of the root: push right (if distinct) then left
+    {
+        BvhNode n;
+        load_node(s, 0, n);
+        int needed = n.child1 == kEmptyChild ? 1 : 2;
+        if (sp + needed > kStackCapacity) { error = 1; hit.slot = -1; return false; }
+        if (n.child1 != kEmptyChild) stack[sp++] = (0 << 1) | 1;
+        stack[sp++] = (0 << 1) | 0;
+    }
+    while (sp) {
+        int32_t entry = stack[--sp];
+        int32_t parent = entry >> 1, side = entry & 1;
+        BvhNode p;
+        load_node(s, parent, p);
+        int32_t child = side ? p.child1 : p.child0;
+        if (child >= 0) {
+            boxes++;
+            float limit = found ? nextafterf(closest, tmax) : tmax;
+            float e;
+            bool h = side ? box_hit(rb, p.c1lox, p.c1hix, p.c1loy, p.c1hiy, p.c1loz, p.c1hiz, tmin, limit, e)
+                          : box_hit(rb, p.c0lox, p.c0hix, p.c0loy, p.c0hiy, p.c0loz, p.c0hiz, tmin, limit, e);
+            if (!h) continue;
+            BvhNode n;
+            load_node(s, child, n);
+            int needed = n.child1 == kEmptyChild ? 1 : 2;
+            if (sp + needed > kStackCapacity) { error = 1; hit.slot = -1; return false; }
+            if (n.child1 != kEmptyChild) stack[sp++] = (child << 1) | 1;
+            stack[sp++] = (child << 1) | 0;
+        } else {
+            test_leaf<false>(s, ~child, r, dl, tmin, tmax, tie, found, closest, best_key, hit, prims);
         }
     }
     return found;

@@ -126,6 +126,17 @@ def library() -> C.CDLL:
         "pt_rays_camera": (I, [P, I, I, U64, U64, S, P]),
         "pt_rays_surface": (I, [P, U64, U64, S, P, P, I]),
         "pt_rays_bounce": (I, [P, P, P, S, U64, U64, P, I]),
+        "pt_renderer_create": (I, [P, P, I, I, U64, C.c_uint32, I, I, P]),
+        "pt_renderer_destroy": (I, [P]),
+        "pt_reset": (I, [P, P]),
+        "pt_add_samples": (I, [P, I]),
+        "pt_set_block_shape": (I, [P, I, I]),
+        "pt_get_sums": (I, [P, P, S]),
+        "pt_get_image": (I, [P, P, S]),
+        "pt_get_rng": (I, [P, P, S]),
+        "pt_write_rgba": (I, [P, P, S]),
+        "pt_rgba_image": (I, [P, P, S]),
+        "pt_stats": (I, [P, P, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -386,3 +397,87 @@ def cuda_query_rays(scene: FlatScene, rays: np.ndarray, brute: bool = False) -> 
         return s.query_compat(rays, brute)
     finally:
         s.close()
+
+
+# ---------------------------------------------------------------- progressive renderer
+class CudaRenderer:
+    """class cuda_renderer (src/cuda/cuda_renderer.h:10-29) on the wavefront kernels.
+
+    ``CudaRenderer(scene, camera, width, height, seed, brute=False, debug=DEBUG_SHADED,
+    direct_light=True, max_depth=50)``: the reference's constructor arguments plus the bounce
+    limit, which the reference hard-codes to 50 (src/renderer/transport.h:174).  ``scene`` is a
+    FlatScene (uploaded and owned by the renderer) or a device ``Scene`` (borrowed).
+    """
+
+    def __init__(self, scene, camera, width: int, height: int, seed: int, brute: bool = False,
+                 debug: int = DEBUG_SHADED, direct_light: bool = True, max_depth: int = 50):
+        self._scene = scene if isinstance(scene, Scene) else Scene(scene)
+        self.width, self.height = int(width), int(height)
+        self._h = C.c_void_p()
+        flags = (RENDER_MIS if direct_light else 0) | (RENDER_BRUTE if brute else 0)
+        cam = np.ascontiguousarray(camera, CAMERA)
+        check(library().pt_renderer_create(self._scene.handle, cam.ctypes.data, self.width, self.height, seed, flags,
+                                           debug, max_depth, C.byref(self._h)))
+
+    @property
+    def pixels(self) -> int:
+        return self.width * self.height
+
+    def close(self):
+        if self._h:
+            library().pt_renderer_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def reset(self, camera) -> None:
+        cam = np.ascontiguousarray(camera, CAMERA)
+        check(library().pt_reset(self._h, cam.ctypes.data))
+
+    def add_samples(self, count: int) -> None:
+        check(library().pt_add_samples(self._h, int(count)))
+
+    def set_block_shape(self, width: int, height: int) -> None:
+        check(library().pt_set_block_shape(self._h, width, height))
+
+    def sums(self) -> np.ndarray:
+        """Linear FP32 radiance sums, 3 per pixel, not divided by the sample count."""
+        out = np.zeros(self.pixels * 3, np.float32)
+        check(library().pt_get_sums(self._h, out.ctypes.data, out.size))
+        return out
+
+    def image(self) -> np.ndarray:
+        out = np.zeros(self.pixels * 3, np.float32)
+        check(library().pt_get_image(self._h, out.ctypes.data, out.size))
+        return out
+
+    def rng_state(self) -> np.ndarray:
+        out = np.zeros(self.pixels * 2, np.uint64)
+        check(library().pt_get_rng(self._h, out.ctypes.data, out.size))
+        return out
+
+    def rgba_image(self) -> np.ndarray:
+        out = np.zeros(self.pixels * 4, np.uint8)
+        check(library().pt_rgba_image(self._h, out.ctypes.data, out.size))
+        return out
+
+    def write_rgba(self, device_pixels, nbytes: int) -> None:
+        check(library().pt_write_rgba(self._h, _ptr(device_pixels), nbytes))
+
+    def _stats(self):
+        s, ms, r = C.c_int(), C.c_float(), C.c_uint64()
+        check(library().pt_stats(self._h, C.byref(s), C.byref(ms), C.byref(r)))
+        return s.value, ms.value, r.value
+
+    def sample_count(self) -> int:
+        return self._stats()[0]
+
+    def kernel_milliseconds(self) -> float:
+        return self._stats()[1]
+
+    def rays_traced(self) -> int:
+        return self._stats()[2]

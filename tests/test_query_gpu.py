@@ -41,19 +41,32 @@ def assert_hits_equal(got, want):
     assert not got["error"].any()
 
 
+def assert_trace_results(got, want):
+    """Bitwise on every field, except the sphere UVs: those come from atan2f/asinf
+    (get_sphere_uv, src/geometry/sphere_uv.h:7-13), whose CUDA and glibc results differ by a few
+    ULP; the reference's own GPU build shows the same difference against its CPU build."""
+    assert np.array_equal(got["hit"], want["hit"]) and np.array_equal(got["error"], want["error"])
+    g, w = got["rec"], want["rec"]
+    for f in ("t", "p", "normal", "material_id", "primitive_type", "primitive_id"):
+        assert g[f].tobytes() == w[f].tobytes(), f
+    sph = w["primitive_type"] == pt.SPHERE_TYPE
+    for f in ("u", "v"):
+        assert g[f][~sph].tobytes() == w[f][~sph].tobytes(), f
+        assert np.allclose(g[f][sph], w[f][sph], rtol=0, atol=1e-6), f
+
+
 @pytest.mark.parametrize("brute", [False, True])
 def test_compat_matches_reference_golden(brute):
     """cuda_query_rays semantics: full 56-byte trace_result, reference tie rule."""
     s = golden_scene("cornell")
     got = pt.cuda_query_rays(s, G["cornell_rays"], brute=brute)
-    want = G[f"cornell_result_brute{int(brute)}"]
-    assert got.tobytes() == want.tobytes()
+    assert_trace_results(got, G[f"cornell_result_brute{int(brute)}"])
 
 
 def test_compat_reference_pipeline_scene():
     s = golden_scene("sphere")
     got = pt.cuda_query_rays(s, G["sphere_rays"])
-    assert got.tobytes() == G["sphere_result"].tobytes()
+    assert_trace_results(got, G["sphere_result"])
 
 
 @pytest.mark.parametrize("prefix", ["cornell", "sphere", "light0", "light1"])
