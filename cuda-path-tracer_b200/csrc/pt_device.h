@@ -59,6 +59,10 @@ private:
 void require_device();
 int device_sm_count();
 
+// Tunables of the traversal kernels (pt_query_tuning; the autotuner sets them).
+struct QueryConfig { int persistent = 1; int min_active = 16; int blocks_per_sm = 0; };
+extern QueryConfig g_query_config;
+
 } // namespace ptb
 
 // The scene handle: everything device-resident that queries and renderers read.
@@ -72,6 +76,8 @@ struct pt_scene {
     // host-buffer query workspace (reused between calls)
     ptb::DeviceBuffer work_rays[3], work_tmax[3], work_hits[3], work_stats[3];
     cudaStream_t streams[3] = {nullptr, nullptr, nullptr};
+    ptb::DeviceBuffer ray_counter;          // per-launch ray counters of the persistent query kernel
+    unsigned counter_slot = 0;
     int device = 0;
     ~pt_scene();
 };

@@ -3,6 +3,7 @@
 // Replaces cuda_query_rays / query_rays (src/cuda/cuda_renderer.cu:111-120, 248-260) and the
 // device_scene upload (src/cuda/cuda_renderer.cu:36-54).
 #include <cfloat>
+#include <algorithm>
 #include <cstring>
 #include <mutex>
 #include "pt_api_common.h"
@@ -49,6 +50,25 @@ __global__ void __launch_bounds__(kQueryBlock) query_kernel(DeviceScene s, const
     int4 out = make_int4(__float_as_int(hit ? h.t : 0.0f), id, type, error);
     reinterpret_cast<int4 *>(hits)[i] = out;
     if(kStats) { stats[i].boxes = boxes; stats[i].primitives = prims; }
+}
+
+// Persistent form: a fixed grid of warps; each warp takes rays from a global counter and,
+// between traversal steps, hands a new ray to every lane whose ray has ended once fewer than
+// `min_active` lanes are still busy.  next_ray must be zero at launch.
+template <bool kAny, bool kStats>
+__global__ void __launch_bounds__(kQueryBlock) query_persistent_kernel(DeviceScene s, const pt_ray *__restrict__ rays, size_t count,
+                                                                       float tmin, const float *__restrict__ tmax,
+                                                                       pt_hit *__restrict__ hits, pt_ray_stats *__restrict__ stats,
+                                                                       int tie, unsigned long long *next_ray, int min_active) {
+    persistent_walk<kAny>(s, count, next_ray, min_active, tie,
+        [&](size_t k, pt_ray &r, float &lo, float &hi) { r = rays[k]; lo = tmin; hi = tmax ? tmax[k] : FLT_MAX; },
+        [&](size_t k, const WalkResult &w) {
+            bool hit = w.slot >= 0;
+            int32_t type = PT_BRANCH, id = -1;
+            if (hit) hit_ids(s, w.slot, type, id);
+            reinterpret_cast<int4 *>(hits)[k] = make_int4(__float_as_int(hit ? w.t : 0.0f), id, type, w.error);
+            if (kStats) { stats[k].boxes = w.boxes; stats[k].primitives = w.prims; }
+        });
 }
 
 template <bool kAny, bool kStats>
@@ -119,11 +139,39 @@ __global__ void bounce_rays_kernel(DeviceScene s, const pt_ray *primary, const p
 
 unsigned grid_for(size_t count, int block) { return unsigned((count + size_t(block) - 1) / size_t(block)); }
 
+// Query kernel variant and its tunables (the autotuner sets these).
+QueryConfig g_query_config;
+
 void launch_query(const pt_scene *sc, const pt_ray *rays, size_t count, int mode, float tmin, const float *tmax,
                   pt_hit *hits, pt_ray_stats *stats, int tie, cudaStream_t stream) {
     if(!count) return;
-    unsigned grid = grid_for(count, kQueryBlock);
     const DeviceScene &s = sc->view;
+    if(g_query_config.persistent) {
+        pt_scene *m = const_cast<pt_scene *>(sc);
+        if(!m->ray_counter.bytes()) m->ray_counter.resize(sizeof(unsigned long long) * 64);
+        unsigned long long *counter = m->ray_counter.get<unsigned long long>() + (m->counter_slot++ % 64);
+        PT_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), stream));
+        static int per_sm[4] = {0, 0, 0, 0};
+        int k = (mode == PT_QUERY_ANY ? 2 : 0) + (stats ? 1 : 0);
+        const void *fn = mode == PT_QUERY_ANY ? (stats ? (const void *)query_persistent_kernel<true, true> : (const void *)query_persistent_kernel<true, false>)
+                                              : (stats ? (const void *)query_persistent_kernel<false, true> : (const void *)query_persistent_kernel<false, false>);
+        const size_t smem = size_t(kSharedStack) * kQueryBlock * sizeof(int32_t);
+        if(!per_sm[k]) PT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[k], fn, kQueryBlock, smem));
+        int bps = g_query_config.blocks_per_sm > 0 ? std::min(g_query_config.blocks_per_sm, per_sm[k]) : per_sm[k];
+        size_t want = (count + kQueryBlock - 1) / kQueryBlock;
+        unsigned grid = unsigned(std::min<size_t>(want, size_t(device_sm_count()) * size_t(bps > 0 ? bps : 1)));
+        int ma = g_query_config.min_active;
+        if(mode == PT_QUERY_ANY) {
+            if(stats) query_persistent_kernel<true, true><<<grid, kQueryBlock, smem, stream>>>(s, rays, count, tmin, tmax, hits, stats, tie, counter, ma);
+            else query_persistent_kernel<true, false><<<grid, kQueryBlock, smem, stream>>>(s, rays, count, tmin, tmax, hits, stats, tie, counter, ma);
+        } else {
+            if(stats) query_persistent_kernel<false, true><<<grid, kQueryBlock, smem, stream>>>(s, rays, count, tmin, tmax, hits, stats, tie, counter, ma);
+            else query_persistent_kernel<false, false><<<grid, kQueryBlock, smem, stream>>>(s, rays, count, tmin, tmax, hits, stats, tie, counter, ma);
+        }
+        PT_CUDA(cudaGetLastError());
+        return;
+    }
+    unsigned grid = grid_for(count, kQueryBlock);
     if(mode == PT_QUERY_ANY) {
         if(stats) query_kernel<true, true><<<grid, kQueryBlock, 0, stream>>>(s, rays, count, tmin, tmax, hits, stats, tie);
         else query_kernel<true, false><<<grid, kQueryBlock, 0, stream>>>(s, rays, count, tmin, tmax, hits, stats, tie);
@@ -313,6 +361,17 @@ pt_status pt_query_rays_compat(const pt_scene *scene, const pt_ray *rays, size_t
         PT_CUDA(cudaGetLastError());
         PT_CUDA(cudaDeviceSynchronize());
         PT_CUDA(cudaMemcpy(results, out.get(), count * sizeof(pt_trace_result), cudaMemcpyDeviceToHost));
+    });
+}
+
+// Query-kernel tuning knobs: persistent (1) or one-thread-per-ray (0) launch, the busy-lane
+// count below which a persistent warp refills, and blocks per SM (0 = occupancy limit).
+pt_status pt_query_tuning(int persistent, int min_active, int blocks_per_sm) {
+    return guard([&]() {
+        if(min_active < 1 || min_active > 32 || blocks_per_sm < 0) throw Error(PT_INVALID_ARGUMENT, "invalid query tuning");
+        g_query_config.persistent = persistent ? 1 : 0;
+        g_query_config.min_active = min_active;
+        g_query_config.blocks_per_sm = blocks_per_sm;
     });
 }
 

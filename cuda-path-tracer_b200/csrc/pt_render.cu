@@ -13,6 +13,7 @@
 // arithmetic (--fmad=false, the same CUDA math functions) the sums, RNG states and ray count
 // equal the reference renderer's.
 #include <cfloat>
+#include <algorithm>
 #include <cstring>
 #include <vector>
 #include "pt_api_common.h"
@@ -52,6 +53,7 @@ struct RenderBuffers {
     int32_t *queue[2];
     int32_t *shadow_queue;
     int32_t *counters;      // [0],[1]: path queues; [2]: shadow queue
+    unsigned long long *fetch;   // [0]: extend's item counter, [1]: shadow's item counter
     unsigned long long *rays;
     int32_t *error;
     float *sums;
@@ -96,7 +98,7 @@ __global__ void init_pixels(float *sums, Pcg *rng, int32_t count, uint64_t seed)
 // First camera ray of every pixel; queue 0 = all pixels in order.
 __global__ void start_samples(RenderParams p, RenderBuffers b, int32_t count, int samples) {
     int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i == 0) { b.counters[0] = count; b.counters[1] = 0; b.counters[2] = 0; }
+    if (i == 0) { b.counters[0] = count; b.counters[1] = 0; b.counters[2] = 0; b.fetch[0] = 0; b.fetch[1] = 0; }
     if (i >= count) return;
     Pcg rng = b.rng[i];
     PathState s;
@@ -116,16 +118,30 @@ __device__ inline pt_ray path_ray(const PathState &s) {
 }
 
 // extend: closest hit of each queued path (trace_color's trace_world, transport.h:177-178)
-__global__ void extend_kernel(DeviceScene scene, RenderParams p, RenderBuffers b, int parity) {
+__global__ void extend_kernel(DeviceScene scene, RenderParams p, RenderBuffers b, int parity, int min_active) {
     const int32_t n = b.counters[parity];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         atomicAdd(b.rays, (unsigned long long)n);
         b.counters[parity ^ 1] = 0;      // the next queue fills during shade
         b.counters[2] = 0;
+        b.fetch[1] = 0;                  // the shadow kernel's item counter
+    }
+    const int32_t *queue = b.queue[parity];
+    if (!p.brute && p.debug != PT_DEBUG_BVH && p.debug != PT_DEBUG_INTERSECTIONS) {
+        persistent_walk<false>(scene, size_t(n), &b.fetch[0], min_active, kTieLastLeaf,
+            [&](size_t k, pt_ray &r, float &lo, float &hi) { r = path_ray(b.paths[queue[k]]); lo = 0.001f; hi = FLT_MAX; },
+            [&](size_t k, const WalkResult &w) {
+                if (w.error) *b.error = 1;
+                PathHit out;
+                out.t = w.t; out.u = w.u; out.v = w.v;
+                out.slot = w.error ? -2 : w.slot;
+                b.hits[queue[k]] = out;
+            });
+        return;
     }
     const bool reference_order = p.debug == PT_DEBUG_BVH || p.debug == PT_DEBUG_INTERSECTIONS;
     for (int32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        int32_t i = b.queue[parity][k];
+        int32_t i = queue[k];
         PathState s = b.paths[i];
         pt_ray r = path_ray(s);
         HitInfo h;
@@ -133,8 +149,7 @@ __global__ void extend_kernel(DeviceScene scene, RenderParams p, RenderBuffers b
         int error = 0;
         bool hit;
         if (p.brute) hit = traverse_brute<false>(scene, p.brute_order, p.leaves, r, 0.001f, FLT_MAX, kTieLastNode, h, prims);
-        else if (reference_order) hit = traverse_reference(scene, r, 0.001f, FLT_MAX, kTieLastLeaf, h, boxes, prims, error);
-        else hit = traverse<false>(scene, r, 0.001f, FLT_MAX, kTieLastLeaf, h, boxes, prims, error);
+        else hit = traverse_reference(scene, r, 0.001f, FLT_MAX, kTieLastLeaf, h, boxes, prims, error);
         if (error) *b.error = 1;
         PathHit out;
         out.t = h.t; out.u = h.u; out.v = h.v; out.slot = (hit && !error) ? h.slot : (error ? -2 : -1);
@@ -143,109 +158,120 @@ __global__ void extend_kernel(DeviceScene scene, RenderParams p, RenderBuffers b
     }
 }
 
-// shade: the rest of one trace_color iteration (transport.h:179-228)
+// The rest of one trace_color iteration for path i (transport.h:179-228), given its closest
+// hit: emission with its MIS weight, next-event estimation (which may emit a shadow ray),
+// cosine or material scatter; when the sample ends, its radiance is added to the pixel sum and
+// the pixel's next camera ray starts.  Returns whether the path is still live.
+__device__ inline bool shade_path(const DeviceScene &scene, const RenderParams &p, const RenderBuffers &b, int32_t i,
+                                  PathState &s, const PathHit &h, const uint2 &stats, Pcg &rng, ShadowRay &sr, bool &shadow) {
+    shadow = false;
+    f3 radiance = mk(s.rr, s.rg, s.rb);
+    f3 throughput = mk(s.tr, s.tg, s.tb);
+    bool finished = false;
+    if (p.debug == PT_DEBUG_BVH || p.debug == PT_DEBUG_INTERSECTIONS) {
+        float cost = log2f(1.0f + float(p.debug == PT_DEBUG_BVH ? stats.x : stats.y)) / 10.0f;
+        cost = fminf(1, cost);
+        radiance = mk(cost, cost * cost, 1 - cost);
+        finished = true;
+    } else if (h.slot < 0) {
+        finished = true;                       // miss, or a traversal error
+    } else {
+        pt_ray r = path_ray(s);
+        HitInfo hi; hi.t = h.t; hi.u = h.u; hi.v = h.v; hi.slot = h.slot;
+        pt_flat_hit rec;
+        finalize_hit(scene, r, hi, rec);
+        if (p.debug == PT_DEBUG_NORMALS) { radiance = 0.5f * (mk(rec.normal) + mk(1, 1, 1)); finished = true; }
+        else if (p.debug == PT_DEBUG_TRIANGLE) {
+            radiance = rec.primitive_type == PT_TRIANGLE ? id_color(rec.primitive_id) : mk(0.3f, 0.3f, 0.3f);
+            finished = true;
+        } else if (p.debug == PT_DEBUG_MATERIAL) { radiance = id_color(rec.material_id); finished = true; }
+        else {
+            const pt_material mat = scene.materials[rec.material_id];
+            f3 in_dir = mk(s.dx, s.dy, s.dz);
+            f3 pos = mk(rec.p), normal = mk(rec.normal);
+            if (mat.type == PT_LIGHT) {
+                float weight = s.prev_pdf > 0 ? mis_weight(s.prev_pdf, hit_light_pdf(scene, mk(s.ox, s.oy, s.oz), rec)) : 1;
+                radiance = radiance + weight * throughput * trace_texture(scene, mat.texture_id, rec.u, rec.v);
+                finished = true;
+            } else if (s.depth == p.max_depth) {
+                finished = true;
+            } else if (p.mis && mat.type == PT_DIFFUSE) {
+                f3 attenuation = trace_texture(scene, mat.texture_id, rec.u, rec.v);
+                if (scene.light_count) {
+                    LightSample light = sample_light(scene, rng);
+                    f3 delta = light.point - pos;
+                    float distance = length(delta);
+                    if (distance > 0.002f && finite(distance)) {
+                        f3 direction = delta / distance;
+                        float cosine = fmaxf(0, dot(normal, direction));
+                        float pdf = light_direction_pdf(scene.light_area, pos, light.point, light.normal);
+                        if (cosine > 0 && pdf > 0) {
+                            const pt_material &emitter = scene.materials[light.material];
+                            f3 emission = trace_texture(scene, emitter.texture_id, light.u, light.v);
+                            float bsdf_pdf = cosine / float(M_PI);
+                            f3 c = throughput * attenuation * emission * (bsdf_pdf * mis_weight(pdf, bsdf_pdf) / pdf);
+                            sr.ox = pos.x; sr.oy = pos.y; sr.oz = pos.z; sr.tmax = distance - 0.001f;
+                            sr.dx = direction.x; sr.dy = direction.y; sr.dz = direction.z; sr.time = s.time;
+                            sr.cr = c.x; sr.cg = c.y; sr.cb = c.z; sr.pixel = i;
+                            shadow = true;
+                        }
+                    }
+                }
+                f3 direction = cosine_direction(normal, rng);
+                s.prev_pdf = fmaxf(0, dot(normal, direction)) / float(M_PI);
+                throughput = throughput * attenuation;
+                s.ox = pos.x; s.oy = pos.y; s.oz = pos.z;
+                s.dx = direction.x; s.dy = direction.y; s.dz = direction.z;
+                s.depth++;
+            } else {
+                s.prev_pdf = 0;
+                f3 attenuation, dir;
+                if (!trace_scatter(scene, mat, in_dir, rec, rng, attenuation, dir)) finished = true;
+                else {
+                    throughput = throughput * attenuation;
+                    s.ox = pos.x; s.oy = pos.y; s.oz = pos.z;
+                    s.dx = dir.x; s.dy = dir.y; s.dz = dir.z;
+                    s.depth++;
+                }
+            }
+        }
+    }
+    if (finished) {
+        // accumulated += trace_pixel_sample(...) (src/cuda/cuda_renderer.cu:81)
+        float *sum = b.sums + 3 * size_t(i);
+        sum[0] = sum[0] + radiance.x; sum[1] = sum[1] + radiance.y; sum[2] = sum[2] + radiance.z;
+        s.samples_left--;
+        if (s.samples_left > 0) {
+            int left = s.samples_left;
+            camera_path(p, i, rng, s);
+            s.samples_left = left;
+            return true;
+        }
+        return false;
+    }
+    s.tr = throughput.x; s.tg = throughput.y; s.tb = throughput.z;
+    s.rr = radiance.x; s.rg = radiance.y; s.rb = radiance.z;
+    return true;
+}
+
+// shade: shade_path over the queue; live paths and shadow rays are appended (warp-aggregated)
 __global__ void shade_kernel(DeviceScene scene, RenderParams p, RenderBuffers b, int parity) {
     const int32_t n = b.counters[parity];
     const int32_t *in = b.queue[parity];
     int32_t *out = b.queue[parity ^ 1];
+    if (blockIdx.x == 0 && threadIdx.x == 0) b.fetch[0] = 0;   // extend's item counter, for the next iteration
     for (int32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
         int32_t k = base + threadIdx.x;
         bool valid = k < n;
         bool live = false, shadow = false;
         int32_t i = valid ? in[k] : 0;
-        ShadowRay sr;
         if (valid) {
             PathState s = b.paths[i];
             PathHit h = b.hits[i];
+            uint2 st = (p.debug == PT_DEBUG_BVH || p.debug == PT_DEBUG_INTERSECTIONS) ? b.stats[i] : make_uint2(0, 0);
             Pcg rng = b.rng[i];
-            f3 radiance = mk(s.rr, s.rg, s.rb);
-            f3 throughput = mk(s.tr, s.tg, s.tb);
-            bool finished = false;
-            if (p.debug == PT_DEBUG_BVH || p.debug == PT_DEBUG_INTERSECTIONS) {
-                uint2 st = b.stats[i];
-                float cost = log2f(1.0f + float(p.debug == PT_DEBUG_BVH ? st.x : st.y)) / 10.0f;
-                cost = fminf(1, cost);
-                radiance = mk(cost, cost * cost, 1 - cost);
-                finished = true;
-            } else if (h.slot < 0) {
-                finished = true;                       // miss, or a traversal error
-            } else {
-                pt_ray r = path_ray(s);
-                HitInfo hi; hi.t = h.t; hi.u = h.u; hi.v = h.v; hi.slot = h.slot;
-                pt_flat_hit rec;
-                finalize_hit(scene, r, hi, rec);
-                if (p.debug == PT_DEBUG_NORMALS) { radiance = 0.5f * (mk(rec.normal) + mk(1, 1, 1)); finished = true; }
-                else if (p.debug == PT_DEBUG_TRIANGLE) {
-                    radiance = rec.primitive_type == PT_TRIANGLE ? id_color(rec.primitive_id) : mk(0.3f, 0.3f, 0.3f);
-                    finished = true;
-                } else if (p.debug == PT_DEBUG_MATERIAL) { radiance = id_color(rec.material_id); finished = true; }
-                else {
-                    const pt_material mat = scene.materials[rec.material_id];
-                    f3 in_dir = mk(s.dx, s.dy, s.dz);
-                    f3 pos = mk(rec.p), normal = mk(rec.normal);
-                    if (mat.type == PT_LIGHT) {
-                        float weight = s.prev_pdf > 0 ? mis_weight(s.prev_pdf, hit_light_pdf(scene, mk(s.ox, s.oy, s.oz), rec)) : 1;
-                        radiance = radiance + weight * throughput * trace_texture(scene, mat.texture_id, rec.u, rec.v);
-                        finished = true;
-                    } else if (s.depth == p.max_depth) {
-                        finished = true;
-                    } else if (p.mis && mat.type == PT_DIFFUSE) {
-                        f3 attenuation = trace_texture(scene, mat.texture_id, rec.u, rec.v);
-                        if (scene.light_count) {
-                            LightSample light = sample_light(scene, rng);
-                            f3 delta = light.point - pos;
-                            float distance = length(delta);
-                            if (distance > 0.002f && finite(distance)) {
-                                f3 direction = delta / distance;
-                                float cosine = fmaxf(0, dot(normal, direction));
-                                float pdf = light_direction_pdf(scene.light_area, pos, light.point, light.normal);
-                                if (cosine > 0 && pdf > 0) {
-                                    const pt_material &emitter = scene.materials[light.material];
-                                    f3 emission = trace_texture(scene, emitter.texture_id, light.u, light.v);
-                                    float bsdf_pdf = cosine / float(M_PI);
-                                    f3 c = throughput * attenuation * emission * (bsdf_pdf * mis_weight(pdf, bsdf_pdf) / pdf);
-                                    sr.ox = pos.x; sr.oy = pos.y; sr.oz = pos.z; sr.tmax = distance - 0.001f;
-                                    sr.dx = direction.x; sr.dy = direction.y; sr.dz = direction.z; sr.time = s.time;
-                                    sr.cr = c.x; sr.cg = c.y; sr.cb = c.z; sr.pixel = i;
-                                    shadow = true;
-                                }
-                            }
-                        }
-                        f3 direction = cosine_direction(normal, rng);
-                        s.prev_pdf = fmaxf(0, dot(normal, direction)) / float(M_PI);
-                        throughput = throughput * attenuation;
-                        s.ox = pos.x; s.oy = pos.y; s.oz = pos.z;
-                        s.dx = direction.x; s.dy = direction.y; s.dz = direction.z;
-                        s.depth++;
-                    } else {
-                        s.prev_pdf = 0;
-                        f3 attenuation, dir;
-                        if (!trace_scatter(scene, mat, in_dir, rec, rng, attenuation, dir)) finished = true;
-                        else {
-                            throughput = throughput * attenuation;
-                            s.ox = pos.x; s.oy = pos.y; s.oz = pos.z;
-                            s.dx = dir.x; s.dy = dir.y; s.dz = dir.z;
-                            s.depth++;
-                        }
-                    }
-                }
-            }
-            if (finished) {
-                // accumulated += trace_pixel_sample(...) (src/cuda/cuda_renderer.cu:81)
-                float *sum = b.sums + 3 * size_t(i);
-                sum[0] = sum[0] + radiance.x; sum[1] = sum[1] + radiance.y; sum[2] = sum[2] + radiance.z;
-                s.samples_left--;
-                if (s.samples_left > 0) {
-                    int left = s.samples_left;
-                    camera_path(p, i, rng, s);
-                    s.samples_left = left;
-                    live = true;
-                }
-            } else {
-                s.tr = throughput.x; s.tg = throughput.y; s.tb = throughput.z;
-                s.rr = radiance.x; s.rg = radiance.y; s.rb = radiance.z;
-                live = true;
-            }
+            ShadowRay sr;
+            live = shade_path(scene, p, b, i, s, h, st, rng, sr, shadow);
             b.paths[i] = s;
             b.rng[i] = rng;
             if (shadow) b.shadows[i] = sr;
@@ -255,10 +281,80 @@ __global__ void shade_kernel(DeviceScene scene, RenderParams p, RenderBuffers b,
     }
 }
 
+// finish: the queue's remaining paths run to the end of their pixel's samples, one thread per
+// path (the reference's megakernel form).  Used once the queue is short, where a wavefront
+// iteration would cost the latency of its slowest ray for a handful of rays.
+__global__ void finish_kernel(DeviceScene scene, RenderParams p, RenderBuffers b, int parity) {
+    const int32_t n = b.counters[parity];
+    const bool reference_order = p.debug == PT_DEBUG_BVH || p.debug == PT_DEBUG_INTERSECTIONS;
+    unsigned long long rays = 0;
+    for (int32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        int32_t i = b.queue[parity][k];
+        PathState s = b.paths[i];
+        Pcg rng = b.rng[i];
+        for (;;) {
+            rays++;   // each closest-hit query counts once, as trace_color counts it (transport.h:177)
+            pt_ray r = path_ray(s);
+            HitInfo hi;
+            uint32_t boxes = 0, prims = 0;
+            int error = 0;
+            bool hit;
+            if (p.brute) hit = traverse_brute<false>(scene, p.brute_order, p.leaves, r, 0.001f, FLT_MAX, kTieLastNode, hi, prims);
+            else if (reference_order) hit = traverse_reference(scene, r, 0.001f, FLT_MAX, kTieLastLeaf, hi, boxes, prims, error);
+            else hit = traverse<false>(scene, r, 0.001f, FLT_MAX, kTieLastLeaf, hi, boxes, prims, error);
+            if (error) *b.error = 1;
+            PathHit h;
+            h.t = hi.t; h.u = hi.u; h.v = hi.v; h.slot = (hit && !error) ? hi.slot : (error ? -2 : -1);
+            ShadowRay sr;
+            bool shadow = false;
+            bool live = shade_path(scene, p, b, i, s, h, make_uint2(boxes, prims), rng, sr, shadow);
+            if (shadow) {
+                rays++;
+                pt_ray q;
+                q.origin = pt_vec3{sr.ox, sr.oy, sr.oz};
+                q.direction = pt_vec3{sr.dx, sr.dy, sr.dz};
+                q.time = sr.time;
+                HitInfo sh;
+                uint32_t sb = 0, spr = 0;
+                int serr = 0;
+                bool blocked = p.brute ? traverse_brute<true>(scene, p.brute_order, p.leaves, q, 0.001f, sr.tmax, kTieLastNode, sh, spr)
+                                       : traverse<true>(scene, q, 0.001f, sr.tmax, kTieLastLeaf, sh, sb, spr, serr);
+                if (serr) *b.error = 1;
+                else if (!blocked) { s.rr = s.rr + sr.cr; s.rg = s.rg + sr.cg; s.rb = s.rb + sr.cb; }
+            }
+            if (!live) break;
+        }
+        b.paths[i] = s;
+        b.rng[i] = rng;
+    }
+    // one add per warp
+    for (int o = 16; o; o >>= 1) rays += __shfl_down_sync(0xffffffffu, rays, o);
+    if ((threadIdx.x & 31) == 0 && rays) atomicAdd(b.rays, rays);
+}
+
 // shadow: any-hit of the NEE rays (transport.h:206-214); unoccluded ones add their contribution
-__global__ void shadow_kernel(DeviceScene scene, RenderParams p, RenderBuffers b) {
+__global__ void shadow_kernel(DeviceScene scene, RenderParams p, RenderBuffers b, int min_active) {
     const int32_t n = b.counters[2];
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(b.rays, (unsigned long long)n);
+    auto add = [&](int32_t i, const ShadowRay &sr) {
+        PathState &s = b.paths[i];
+        s.rr = s.rr + sr.cr; s.rg = s.rg + sr.cg; s.rb = s.rb + sr.cb;
+    };
+    if (!p.brute) {
+        persistent_walk<true>(scene, size_t(n), &b.fetch[1], min_active, kTieLastLeaf,
+            [&](size_t k, pt_ray &r, float &lo, float &hi) {
+                const ShadowRay &sr = b.shadows[b.shadow_queue[k]];
+                r.origin = pt_vec3{sr.ox, sr.oy, sr.oz};
+                r.direction = pt_vec3{sr.dx, sr.dy, sr.dz};
+                r.time = sr.time;
+                lo = 0.001f; hi = sr.tmax;
+            },
+            [&](size_t k, const WalkResult &w) {
+                if (w.error) { *b.error = 1; return; }
+                if (w.slot < 0) { int32_t i = b.shadow_queue[k]; add(i, b.shadows[i]); }
+            });
+        return;
+    }
     for (int32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         int32_t i = b.shadow_queue[k];
         ShadowRay sr = b.shadows[i];
@@ -267,15 +363,9 @@ __global__ void shadow_kernel(DeviceScene scene, RenderParams p, RenderBuffers b
         r.direction = pt_vec3{sr.dx, sr.dy, sr.dz};
         r.time = sr.time;
         HitInfo h;
-        uint32_t boxes = 0, prims = 0;
-        int error = 0;
-        bool blocked = p.brute ? traverse_brute<true>(scene, p.brute_order, p.leaves, r, 0.001f, sr.tmax, kTieLastNode, h, prims)
-                               : traverse<true>(scene, r, 0.001f, sr.tmax, kTieLastLeaf, h, boxes, prims, error);
-        if (error) { *b.error = 1; continue; }
-        if (!blocked) {
-            PathState &s = b.paths[i];
-            s.rr = s.rr + sr.cr; s.rg = s.rg + sr.cg; s.rb = s.rb + sr.cb;
-        }
+        uint32_t prims = 0;
+        bool blocked = traverse_brute<true>(scene, p.brute_order, p.leaves, r, 0.001f, sr.tmax, kTieLastNode, h, prims);
+        if (!blocked) add(i, sr);
     }
 }
 
@@ -292,9 +382,11 @@ __global__ void pack_pixels(const float *sum, unsigned char *rgba, size_t count,
     rgba[4 * i + 3] = 255;
 }
 
-int occupancy_grid(const void *kernel, int block) {
+size_t stack_bytes(int block) { return size_t(kSharedStack) * size_t(block) * sizeof(int32_t); }
+
+int occupancy_grid(const void *kernel, int block, size_t smem = 0) {
     int per_sm = 0;
-    PT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0));
+    PT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, smem));
     return device_sm_count() * (per_sm > 0 ? per_sm : 1);
 }
 
@@ -309,8 +401,9 @@ struct pt_renderer {
     float milliseconds = 0;
     uint64_t rays = 0;
     int block = 256;
-    int grid_extend = 0, grid_shade = 0, grid_shadow = 0;
-    DeviceBuffer paths, hits, stats, shadows, queue0, queue1, shadow_queue, counters, ray_total, error, sums, rng, rgba;
+    int grid_extend = 0, grid_shade = 0, grid_shadow = 0, grid_finish = 0;
+    int32_t tail_paths = 0;             // live-path count below which the fused finish kernel takes over
+    DeviceBuffer paths, hits, stats, shadows, queue0, queue1, shadow_queue, counters, fetch, ray_total, error, sums, rng, rgba;
     RenderBuffers buf{};
     cudaStream_t stream = nullptr;
     Event start, stop;
@@ -321,9 +414,10 @@ struct pt_renderer {
         if (stream) cudaStreamDestroy(stream);
     }
     void grids() {
-        grid_extend = occupancy_grid((const void *)extend_kernel, block);
+        grid_extend = occupancy_grid((const void *)extend_kernel, block, stack_bytes(block));
         grid_shade = occupancy_grid((const void *)shade_kernel, block);
-        grid_shadow = occupancy_grid((const void *)shadow_kernel, block);
+        grid_shadow = occupancy_grid((const void *)shadow_kernel, block, stack_bytes(block));
+        grid_finish = occupancy_grid((const void *)finish_kernel, block);
     }
 };
 
@@ -371,6 +465,7 @@ pt_status pt_renderer_create(const pt_scene *scene, const pt_camera *camera, int
             r->queue1.resize(n * sizeof(int32_t));
             r->shadow_queue.resize(n * sizeof(int32_t));
             r->counters.resize(4 * sizeof(int32_t));
+            r->fetch.resize(2 * sizeof(unsigned long long));
             r->ray_total.resize(sizeof(unsigned long long));
             r->error.resize(sizeof(int32_t));
             r->sums.resize(n * 3 * sizeof(float));
@@ -380,11 +475,13 @@ pt_status pt_renderer_create(const pt_scene *scene, const pt_camera *camera, int
             b.shadows = r->shadows.get<ShadowRay>();
             b.queue[0] = r->queue0.get<int32_t>(); b.queue[1] = r->queue1.get<int32_t>();
             b.shadow_queue = r->shadow_queue.get<int32_t>(); b.counters = r->counters.get<int32_t>();
+            b.fetch = r->fetch.get<unsigned long long>();
             b.rays = r->ray_total.get<unsigned long long>(); b.error = r->error.get<int32_t>();
             b.sums = r->sums.get<float>(); b.rng = r->rng.get<Pcg>();
             PT_CUDA(cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking));
             PT_CUDA(cudaMallocHost(&r->host_counters, kIterationRing * sizeof(int32_t)));
             r->grids();
+            r->tail_paths = std::max<int32_t>(16384, r->pixels / 16);
         } catch (...) { delete r; throw; }
         *out = r;
         pt_status st = pt_reset(r, camera);
@@ -424,11 +521,11 @@ pt_status pt_add_samples(pt_renderer *r, int count) {
         const int64_t max_iterations = int64_t(count) * (int64_t(r->params.max_depth) + 1) + 1;
         int parity = 0;
         int64_t issued = 0, checked = 0;
-        bool done = false;
-        while (!done && issued < max_iterations) {
-            extend_kernel<<<r->grid_extend, r->block, 0, st>>>(scene, r->params, r->buf, parity);
+        bool done = false, tail = false;
+        while (!done && !tail && issued < max_iterations) {
+            extend_kernel<<<r->grid_extend, r->block, stack_bytes(r->block), st>>>(scene, r->params, r->buf, parity, g_query_config.min_active);
             shade_kernel<<<r->grid_shade, r->block, 0, st>>>(scene, r->params, r->buf, parity);
-            shadow_kernel<<<r->grid_shadow, r->block, 0, st>>>(scene, r->params, r->buf);
+            shadow_kernel<<<r->grid_shadow, r->block, stack_bytes(r->block), st>>>(scene, r->params, r->buf, g_query_config.min_active);
             PT_CUDA(cudaGetLastError());
             parity ^= 1;
             int slot = int(issued % kIterationRing);
@@ -439,9 +536,17 @@ pt_status pt_add_samples(pt_renderer *r, int count) {
             while (checked < issued && (issued - checked >= kIterationRing / 2 ||
                                         cudaEventQuery(r->iteration_events[int(checked % kIterationRing)].get()) == cudaSuccess)) {
                 PT_CUDA(cudaEventSynchronize(r->iteration_events[int(checked % kIterationRing)].get()));
-                if (r->host_counters[int(checked % kIterationRing)] == 0) { done = true; break; }
+                int32_t live = r->host_counters[int(checked % kIterationRing)];
+                if (live == 0) { done = true; break; }
+                if (live < r->tail_paths) { tail = true; break; }
                 checked++;
             }
+        }
+        if (tail && !done) {
+            // the few remaining paths (of the last issued iteration's queue) run to completion
+            finish_kernel<<<r->grid_finish, r->block, 0, st>>>(scene, r->params, r->buf, parity);
+            PT_CUDA(cudaGetLastError());
+            done = true;
         }
         while (!done && checked < issued) {   // iterations issued but not yet inspected
             PT_CUDA(cudaEventSynchronize(r->iteration_events[int(checked % kIterationRing)].get()));
@@ -461,6 +566,15 @@ pt_status pt_add_samples(pt_renderer *r, int count) {
         r->milliseconds += ms;
         r->samples += count;
         r->rays += total;
+    });
+}
+
+// Live-path count below which add_samples hands the remaining paths to the fused finish kernel
+// (0: wavefront to the end; INT32_MAX: fused kernel from the first iteration).
+pt_status pt_renderer_tuning(pt_renderer *r, int32_t tail_paths) {
+    return guard([&]() {
+        if (!r || tail_paths < 0) throw Error(PT_INVALID_ARGUMENT, "invalid renderer tuning");
+        r->tail_paths = tail_paths;
     });
 }
 

@@ -294,3 +294,201 @@ PT_HD inline void hit_ids(const DeviceScene &s, int32_t slot, int32_t &type, int
 }
 
 } // namespace ptb
+
+namespace ptb {
+
+// Resumable closest-hit / any-hit traversal: the same walk as traverse<>, cut into steps of
+// one node each so a persistent warp can retire finished rays and take new ones between
+// steps (the lanes of a warp then stay busy until the ray pool is empty).
+struct Walker {
+    RayBox rb;
+    pt_ray r;
+    float dl, tmin, tmax, closest;
+    long long best_key;
+    HitInfo hit;
+    uint32_t boxes, prims;
+    int32_t node, sp;
+    bool found;
+    int error;
+    int32_t stack[kStackCapacity];
+
+    PT_HD void begin(const DeviceScene &s, const pt_ray &ray, float lo, float hi) {
+        r = ray; rb = ray_box(ray); dl = length(mk(ray.direction));
+        tmin = lo; tmax = hi; closest = hi; best_key = 0;
+        hit.slot = -1; hit.t = 0; hit.u = 0; hit.v = 0;
+        boxes = 0; prims = 0; sp = 0; found = false; error = 0;
+        node = (s.empty || s.node_count == 0) ? -1 : 0;
+    }
+    // One node: both child boxes, leaf children tested at once (nearer first), descend into
+    // the nearer inner child and push the other.  Returns true when the walk has ended.
+    template <bool kAny>
+    PT_HD bool step(const DeviceScene &s, int tie) {
+        if (node < 0) return true;
+        BvhNode n;
+        load_node(s, node, n);
+        float limit = found ? nextafterf(closest, tmax) : tmax;
+        float e0, e1;
+        bool h0 = n.child0 != kEmptyChild && box_hit(rb, n.c0lox, n.c0hix, n.c0loy, n.c0hiy, n.c0loz, n.c0hiz, tmin, limit, e0);
+        bool h1 = n.child1 != kEmptyChild && box_hit(rb, n.c1lox, n.c1hix, n.c1loy, n.c1hiy, n.c1loz, n.c1hiz, tmin, limit, e1);
+        boxes += (n.child0 != kEmptyChild) + (n.child1 != kEmptyChild);
+        int32_t first = n.child0, second = n.child1;
+        bool hf = h0, hs = h1;
+        if (h0 && h1 && e1 < e0) { first = n.child1; second = n.child0; }
+        else if (!h0) { first = n.child1; hf = h1; hs = false; }
+        int32_t inner[2];
+        int ninner = 0;
+        if (hf) {
+            if (first < 0) {
+                if (test_leaf<kAny>(s, ~first, r, dl, tmin, tmax, tie, found, closest, best_key, hit, prims) && kAny) { node = -1; return true; }
+            } else inner[ninner++] = first;
+        }
+        if (hs) {
+            if (second < 0) {
+                if (test_leaf<kAny>(s, ~second, r, dl, tmin, tmax, tie, found, closest, best_key, hit, prims) && kAny) { node = -1; return true; }
+            } else inner[ninner++] = second;
+        }
+        if (ninner == 2) {
+            if (sp >= kStackCapacity) { error = 1; found = false; hit.slot = -1; node = -1; return true; }
+            stack[sp++] = inner[1];
+            node = inner[0];
+        } else if (ninner == 1) {
+            node = inner[0];
+        } else {
+            if (sp == 0) { node = -1; return true; }
+            node = stack[--sp];
+        }
+        return false;
+    }
+};
+
+} // namespace ptb
+
+#ifdef __CUDACC__
+namespace ptb {
+
+// Entries of each lane's traversal stack kept in shared memory (entry-major, so the lanes of a
+// warp touch consecutive words); deeper entries go to local memory.  A near-first walk pushes
+// at most one entry per level, so a validated tree (depth <= 64) never needs more than 63.
+constexpr int kSharedStack = 32;
+
+// Result of a finished walk, handed to the consumer.
+struct WalkResult { float t, u, v; int32_t slot; uint32_t boxes, prims; int error; };
+
+// Persistent warp loop over `count` work items.  Lanes take item indices from *next (one
+// atomicAdd per warp); between traversal steps a warp hands new items to idle lanes once fewer
+// than `min_active` lanes are busy.  get(k, ray, tmin, tmax) loads item k; done(k, result)
+// consumes a finished walk.  Every lane of the warp must call this together, and the block
+// must provide kSharedStack * blockDim.x int32 words of dynamic shared memory.
+template <bool kAny, class Get, class Done>
+__device__ inline void persistent_walk(const DeviceScene &s, size_t count, unsigned long long *next, int min_active,
+                                       int tie, Get get, Done done) {
+    // Warps past the first `count` lanes have nothing to take: they leave before touching the
+    // shared counter (a short queue then costs a few warps, not the whole resident grid).
+    const size_t warp_first = (size_t(blockIdx.x) * blockDim.x + (threadIdx.x & ~31u));
+    if (warp_first >= count) return;
+    extern __shared__ int32_t shared_stack[];
+    int32_t *my_stack = shared_stack + threadIdx.x;
+    const int stride = blockDim.x;
+    int32_t spill[kStackCapacity - kSharedStack];
+    const unsigned lane = threadIdx.x & 31;
+    // walk state (registers)
+    pt_ray r;
+    RayBox rb;
+    float dl = 0, tmin = 0, tmax = 0, closest = 0;
+    long long best_key = 0;
+    HitInfo hit;
+    uint32_t boxes = 0, prims = 0;
+    int32_t node = -1, sp = 0;
+    bool found = false;
+    int error = 0;
+    size_t index = 0;
+    bool busy = false, pool_empty = false;
+    hit.slot = -1; hit.t = 0; hit.u = 0; hit.v = 0;
+    for (;;) {
+        unsigned idle = __ballot_sync(0xffffffffu, !busy);
+        if (idle && !pool_empty) {
+            int leader = __ffs(idle) - 1;
+            unsigned long long base = 0;
+            if ((int)lane == leader) base = atomicAdd(next, (unsigned long long)__popc(idle));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (base + __popc(idle) >= count) pool_empty = true;
+            if (!busy) {
+                size_t mine = base + __popc(idle & ((1u << lane) - 1u));
+                if (mine < count) {
+                    index = mine;
+                    get(index, r, tmin, tmax);
+                    rb = ray_box(r);
+                    dl = length(mk(r.direction));
+                    closest = tmax; best_key = 0;
+                    hit.slot = -1; hit.t = 0; hit.u = 0; hit.v = 0;
+                    boxes = 0; prims = 0; sp = 0; found = false; error = 0;
+                    node = (s.empty || s.node_count == 0) ? -1 : 0;
+                    busy = true;
+                }
+            }
+        }
+        if (!__any_sync(0xffffffffu, busy)) break;
+        const int threshold = pool_empty ? 1 : min_active;
+        for (;;) {
+            if (busy) {
+                bool end = false;
+                if (node < 0) end = true;
+                else {
+                    BvhNode n;
+                    load_node(s, node, n);
+                    float limit = found ? nextafterf(closest, tmax) : tmax;
+                    float e0, e1;
+                    bool h0 = n.child0 != kEmptyChild && box_hit(rb, n.c0lox, n.c0hix, n.c0loy, n.c0hiy, n.c0loz, n.c0hiz, tmin, limit, e0);
+                    bool h1 = n.child1 != kEmptyChild && box_hit(rb, n.c1lox, n.c1hix, n.c1loy, n.c1hiy, n.c1loz, n.c1hiz, tmin, limit, e1);
+                    boxes += (n.child0 != kEmptyChild) + (n.child1 != kEmptyChild);
+                    int32_t first = n.child0, second = n.child1;
+                    bool hf = h0, hs = h1;
+                    if (h0 && h1 && e1 < e0) { first = n.child1; second = n.child0; }
+                    else if (!h0) { first = n.child1; hf = h1; hs = false; }
+                    int32_t inner0 = -1, inner1 = -1;
+                    int ninner = 0;
+                    if (hf) {
+                        if (first < 0) {
+                            if (test_leaf<kAny>(s, ~first, r, dl, tmin, tmax, tie, found, closest, best_key, hit, prims) && kAny) end = true;
+                        } else { inner0 = first; ninner = 1; }
+                    }
+                    if (hs && !end) {
+                        if (second < 0) {
+                            if (test_leaf<kAny>(s, ~second, r, dl, tmin, tmax, tie, found, closest, best_key, hit, prims) && kAny) end = true;
+                        } else { if (ninner) inner1 = second; else inner0 = second; ninner++; }
+                    }
+                    if (!end) {
+                        if (ninner == 2) {
+                            if (sp >= kStackCapacity) { error = 1; found = false; hit.slot = -1; end = true; }
+                            else {
+                                if (sp < kSharedStack) my_stack[sp * stride] = inner1;
+                                else spill[sp - kSharedStack] = inner1;
+                                sp++;
+                                node = inner0;
+                            }
+                        } else if (ninner == 1) {
+                            node = inner0;
+                        } else if (sp == 0) {
+                            end = true;
+                        } else {
+                            sp--;
+                            node = sp < kSharedStack ? my_stack[sp * stride] : spill[sp - kSharedStack];
+                        }
+                    }
+                }
+                if (end) {
+                    WalkResult res;
+                    res.t = hit.t; res.u = hit.u; res.v = hit.v; res.slot = found ? hit.slot : -1;
+                    res.boxes = boxes; res.prims = prims; res.error = error;
+                    done(index, res);
+                    busy = false;
+                    node = -1;
+                }
+            }
+            if (__popc(__ballot_sync(0xffffffffu, busy)) < threshold) break;
+        }
+    }
+}
+
+} // namespace ptb
+#endif

@@ -113,6 +113,7 @@ def library() -> C.CDLL:
         "pt_query_rays_brute_device": (I, [P, P, S, I, F, P, P, P, P]),
         "pt_query_rays": (I, [P, P, S, I, F, P, P, P]),
         "pt_query_rays_compat": (I, [P, P, S, I, P]),
+        "pt_query_tuning": (I, [I, I, I]),
         "pt_rays_camera_device": (I, [P, I, I, U64, U64, S, P, P]),
         "pt_rays_bounce_device": (I, [P, P, P, S, U64, U64, P, P]),
         "pt_flat_from_desc": (I, [P, P]),
@@ -137,6 +138,7 @@ def library() -> C.CDLL:
         "pt_write_rgba": (I, [P, P, S]),
         "pt_rgba_image": (I, [P, P, S]),
         "pt_stats": (I, [P, P, P, P]),
+        "pt_renderer_tuning": (I, [P, C.c_int32]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -390,6 +392,11 @@ def camera_rays_device(camera: np.ndarray, width, height, seed, first, count, ou
     check(library().pt_rays_camera_device(camera.ctypes.data, width, height, seed, first, count, _ptr(out), stream))
 
 
+def query_tuning(persistent: int = 1, min_active: int = 20, blocks_per_sm: int = 0) -> None:
+    """Sets the ray-query kernel variant and its tunables (pt_query_tuning)."""
+    check(library().pt_query_tuning(persistent, min_active, blocks_per_sm))
+
+
 def cuda_query_rays(scene: FlatScene, rays: np.ndarray, brute: bool = False) -> np.ndarray:
     """cuda_query_rays(scene, rays, brute) (src/cuda/cuda_renderer.cu:248-260): TRACE_RESULT records."""
     s = Scene(scene)
@@ -443,6 +450,10 @@ class CudaRenderer:
 
     def set_block_shape(self, width: int, height: int) -> None:
         check(library().pt_set_block_shape(self._h, width, height))
+
+    def set_tail_paths(self, tail_paths: int) -> None:
+        """Live-path count below which the fused finish kernel takes over (pt_renderer_tuning)."""
+        check(library().pt_renderer_tuning(self._h, int(tail_paths)))
 
     def sums(self) -> np.ndarray:
         """Linear FP32 radiance sums, 3 per pixel, not divided by the sample count."""

@@ -145,6 +145,12 @@ pt_status pt_query_rays_brute_device(const pt_scene *scene, const pt_ray *rays, 
                                      float tmin, const float *tmax, pt_hit *hits, pt_ray_stats *stats,
                                      void *stream);
 
+/* Tuning of the ray-query kernel (process-wide): persistent = 1 runs a fixed grid of warps that
+ * take rays from a global counter and refill lanes whose ray has ended once fewer than
+ * `min_active` (1..32) lanes are busy; persistent = 0 launches one thread per ray.
+ * blocks_per_sm = 0 uses the occupancy limit.  Defaults: 1, 20, 0. */
+pt_status pt_query_tuning(int persistent, int min_active, int blocks_per_sm);
+
 /* ---- device ray generators (bit-identical to the host ones in pt_workloads.h) ----
  * Camera rays of pt_rays_camera; bounce rays from closest hits: origin at the hit, a
  * cosine-distributed direction about the geometric normal turned toward the ray, one PCG stream
@@ -170,6 +176,10 @@ pt_status pt_add_samples(pt_renderer *renderer, int count);
 /* set_block_shape(w, h): accepted shapes 8x8, 16x8, 16x16, 32x8 (src/cuda/cuda_renderer.cu:215-228).
  * Sets the thread-block size of the wavefront kernels to w*h threads. */
 pt_status pt_set_block_shape(pt_renderer *renderer, int width, int height);
+/* Live-path count below which add_samples stops the wavefront and runs the remaining paths to
+ * completion in one fused kernel, one thread per path (default max(16384, pixels/16); 0 keeps the
+ * wavefront to the end).  Results do not depend on it. */
+pt_status pt_renderer_tuning(pt_renderer *renderer, int32_t tail_paths);
 /* Linear FP32 radiance sums (3 floats per pixel, row 0 at the bottom, not divided by spp). */
 pt_status pt_get_sums(const pt_renderer *renderer, float *rgb_sums, size_t floats);
 /* image(): sums / spp (src/cuda/cuda_renderer.cu:230-234). */
