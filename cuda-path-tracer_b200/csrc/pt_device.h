@@ -60,7 +60,7 @@ void require_device();
 int device_sm_count();
 
 // Tunables of the traversal kernels (pt_query_tuning; the autotuner sets them).
-struct QueryConfig { int persistent = 1; int min_active = 16; int blocks_per_sm = 0; };
+struct QueryConfig { int persistent = 1; int min_active = 24; int blocks_per_sm = 0; int wide = 1; };
 extern QueryConfig g_query_config;
 
 } // namespace ptb
@@ -68,7 +68,7 @@ extern QueryConfig g_query_config;
 // The scene handle: everything device-resident that queries and renderers read.
 struct pt_scene {
     ptb::DeviceScene view{};
-    ptb::DeviceBuffer nodes, tris, spheres, triangles, sphere_src, materials, textures, pixels, lights, brute_order;
+    ptb::DeviceBuffer nodes, nodes4, tris, spheres, triangles, sphere_src, materials, textures, pixels, lights, brute_order;
     std::vector<pt_light> host_lights;
     float light_area = 0;
     int32_t leaf_count = 0;

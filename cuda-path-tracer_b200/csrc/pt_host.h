@@ -30,6 +30,7 @@ struct HostLayout {
     int32_t empty = 1;
     float root_lo[3] = {0, 0, 0}, root_hi[3] = {0, 0, 0};
     int32_t root_leaf = 0;
+    std::vector<Bvh4Node> nodes4;       // empty when the flat graph shares subtrees
 };
 HostLayout relayout(const pt_scene_desc &scene);
 

@@ -38,6 +38,17 @@ struct alignas(16) BvhNode {
 };
 static_assert(sizeof(BvhNode) == 64, "node is 64 bytes");
 
+// Four-wide node collapsed from the binary tree: the boxes of up to four children in SoA
+// (x/y/z min and max, four lanes each) and their references.  A child reference >= 0 is another
+// four-wide node; < 0 is a leaf of 1..8 consecutive slots, ~(first_slot << 3 | (count - 1));
+// kEmptyChild marks an unused lane (its box is inverted, so it never passes).
+struct alignas(16) Bvh4Node {
+    float lox[4], hix[4], loy[4], hiy[4], loz[4], hiz[4];
+    int32_t child[4];
+};
+static_assert(sizeof(Bvh4Node) == 112, "four-wide node is 112 bytes");
+constexpr int kLeafMax = 4;   // slots per four-wide leaf
+
 struct alignas(16) TriRecord {
     float v0x, v0y, v0z, eps;
     float e1x, e1y, e1z; int32_t id;
@@ -54,6 +65,7 @@ static_assert(sizeof(SphereRecord) == 32, "sphere record is 32 bytes");
 // Everything a kernel needs, passed by value (device pointers).
 struct DeviceScene {
     const BvhNode *nodes;
+    const Bvh4Node *nodes4;         // null when the tree could not be collapsed (shared subtrees)
     const TriRecord *tris;
     const SphereRecord *spheres;
     const pt_triangle *triangles;   // caller's records (shading, light sampling)

@@ -55,20 +55,21 @@ __global__ void __launch_bounds__(kQueryBlock) query_kernel(DeviceScene s, const
 // Persistent form: a fixed grid of warps; each warp takes rays from a global counter and,
 // between traversal steps, hands a new ray to every lane whose ray has ended once fewer than
 // `min_active` lanes are still busy.  next_ray must be zero at launch.
-template <bool kAny, bool kStats>
+template <bool kAny, bool kStats, bool kWide>
 __global__ void __launch_bounds__(kQueryBlock) query_persistent_kernel(DeviceScene s, const pt_ray *__restrict__ rays, size_t count,
                                                                        float tmin, const float *__restrict__ tmax,
                                                                        pt_hit *__restrict__ hits, pt_ray_stats *__restrict__ stats,
                                                                        int tie, unsigned long long *next_ray, int min_active) {
-    persistent_walk<kAny>(s, count, next_ray, min_active, tie,
-        [&](size_t k, pt_ray &r, float &lo, float &hi) { r = rays[k]; lo = tmin; hi = tmax ? tmax[k] : FLT_MAX; },
-        [&](size_t k, const WalkResult &w) {
-            bool hit = w.slot >= 0;
-            int32_t type = PT_BRANCH, id = -1;
-            if (hit) hit_ids(s, w.slot, type, id);
-            reinterpret_cast<int4 *>(hits)[k] = make_int4(__float_as_int(hit ? w.t : 0.0f), id, type, w.error);
-            if (kStats) { stats[k].boxes = w.boxes; stats[k].primitives = w.prims; }
-        });
+    auto get = [&](size_t k, pt_ray &r, float &lo, float &hi) { r = rays[k]; lo = tmin; hi = tmax ? tmax[k] : FLT_MAX; };
+    auto done = [&](size_t k, const WalkResult &w) {
+        bool hit = w.slot >= 0;
+        int32_t type = PT_BRANCH, id = -1;
+        if (hit) hit_ids(s, w.slot, type, id);
+        reinterpret_cast<int4 *>(hits)[k] = make_int4(__float_as_int(hit ? w.t : 0.0f), id, type, w.error);
+        if (kStats) { stats[k].boxes = w.boxes; stats[k].primitives = w.prims; }
+    };
+    if (kWide) persistent_walk4<kAny>(s, count, next_ray, min_active, tie, get, done);
+    else persistent_walk<kAny>(s, count, next_ray, min_active, tie, get, done);
 }
 
 template <bool kAny, bool kStats>
@@ -151,23 +152,24 @@ void launch_query(const pt_scene *sc, const pt_ray *rays, size_t count, int mode
         if(!m->ray_counter.bytes()) m->ray_counter.resize(sizeof(unsigned long long) * 64);
         unsigned long long *counter = m->ray_counter.get<unsigned long long>() + (m->counter_slot++ % 64);
         PT_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), stream));
-        static int per_sm[4] = {0, 0, 0, 0};
-        int k = (mode == PT_QUERY_ANY ? 2 : 0) + (stats ? 1 : 0);
-        const void *fn = mode == PT_QUERY_ANY ? (stats ? (const void *)query_persistent_kernel<true, true> : (const void *)query_persistent_kernel<true, false>)
-                                              : (stats ? (const void *)query_persistent_kernel<false, true> : (const void *)query_persistent_kernel<false, false>);
-        const size_t smem = size_t(kSharedStack) * kQueryBlock * sizeof(int32_t);
-        if(!per_sm[k]) PT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[k], fn, kQueryBlock, smem));
+        const bool wide = g_query_config.wide && s.nodes4;
+        const bool any = mode == PT_QUERY_ANY;
+        using Fn = void (*)(DeviceScene, const pt_ray *, size_t, float, const float *, pt_hit *, pt_ray_stats *, int,
+                            unsigned long long *, int);
+        static const Fn table[8] = {
+            query_persistent_kernel<false, false, false>, query_persistent_kernel<false, false, true>,
+            query_persistent_kernel<false, true, false>, query_persistent_kernel<false, true, true>,
+            query_persistent_kernel<true, false, false>, query_persistent_kernel<true, false, true>,
+            query_persistent_kernel<true, true, false>, query_persistent_kernel<true, true, true>};
+        int k = (any ? 4 : 0) + (stats ? 2 : 0) + (wide ? 1 : 0);
+        Fn fn = table[k];
+        static int per_sm[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        const size_t smem = wide ? size_t(kSharedStack4) * kQueryBlock * sizeof(int2) : size_t(kSharedStack) * kQueryBlock * sizeof(int32_t);
+        if(!per_sm[k]) PT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[k], (const void *)fn, kQueryBlock, smem));
         int bps = g_query_config.blocks_per_sm > 0 ? std::min(g_query_config.blocks_per_sm, per_sm[k]) : per_sm[k];
         size_t want = (count + kQueryBlock - 1) / kQueryBlock;
         unsigned grid = unsigned(std::min<size_t>(want, size_t(device_sm_count()) * size_t(bps > 0 ? bps : 1)));
-        int ma = g_query_config.min_active;
-        if(mode == PT_QUERY_ANY) {
-            if(stats) query_persistent_kernel<true, true><<<grid, kQueryBlock, smem, stream>>>(s, rays, count, tmin, tmax, hits, stats, tie, counter, ma);
-            else query_persistent_kernel<true, false><<<grid, kQueryBlock, smem, stream>>>(s, rays, count, tmin, tmax, hits, stats, tie, counter, ma);
-        } else {
-            if(stats) query_persistent_kernel<false, true><<<grid, kQueryBlock, smem, stream>>>(s, rays, count, tmin, tmax, hits, stats, tie, counter, ma);
-            else query_persistent_kernel<false, false><<<grid, kQueryBlock, smem, stream>>>(s, rays, count, tmin, tmax, hits, stats, tie, counter, ma);
-        }
+        fn<<<grid, kQueryBlock, smem, stream>>>(s, rays, count, tmin, tmax, hits, stats, tie, counter, g_query_config.min_active);
         PT_CUDA(cudaGetLastError());
         return;
     }
@@ -233,6 +235,7 @@ pt_status pt_scene_create(const pt_scene_desc *desc, pt_scene **out) {
             sc->triangle_count = desc->triangle_count;
             sc->sphere_count = desc->sphere_count;
             sc->nodes.upload(layout.nodes);
+            sc->nodes4.upload(layout.nodes4);
             sc->tris.upload(layout.tris);
             sc->spheres.upload(layout.spheres);
             sc->brute_order.upload(layout.brute_order);
@@ -245,6 +248,7 @@ pt_status pt_scene_create(const pt_scene_desc *desc, pt_scene **out) {
             sc->leaf_count = int32_t(layout.brute_order.size());
             DeviceScene &v = sc->view;
             v.nodes = sc->nodes.get<BvhNode>();
+            v.nodes4 = layout.nodes4.empty() ? nullptr : sc->nodes4.get<Bvh4Node>();
             v.tris = sc->tris.get<TriRecord>();
             v.spheres = sc->spheres.get<SphereRecord>();
             v.triangles = sc->triangles.get<pt_triangle>();
@@ -280,7 +284,7 @@ pt_status pt_scene_lights(const pt_scene *scene, pt_light *lights, size_t capaci
 pt_status pt_scene_device_bytes(const pt_scene *s, size_t *bytes) {
     return guard([&]() {
         if(!s || !bytes) throw Error(PT_INVALID_ARGUMENT, "null argument");
-        *bytes = s->nodes.bytes() + s->tris.bytes() + s->spheres.bytes() + s->triangles.bytes() + s->sphere_src.bytes() +
+        *bytes = s->nodes.bytes() + s->nodes4.bytes() + s->tris.bytes() + s->spheres.bytes() + s->triangles.bytes() + s->sphere_src.bytes() +
                  s->materials.bytes() + s->textures.bytes() + s->pixels.bytes() + s->lights.bytes() + s->brute_order.bytes();
     });
 }
@@ -373,6 +377,11 @@ pt_status pt_query_tuning(int persistent, int min_active, int blocks_per_sm) {
         g_query_config.min_active = min_active;
         g_query_config.blocks_per_sm = blocks_per_sm;
     });
+}
+
+// Node layout of the traversal kernels: 1 = four-wide nodes where the scene has them, 0 = two-wide.
+pt_status pt_query_layout(int wide) {
+    return guard([&]() { g_query_config.wide = wide ? 1 : 0; });
 }
 
 pt_status pt_rays_camera_device(const pt_camera *camera, int width, int height, uint64_t seed, uint64_t first,

@@ -40,7 +40,7 @@ static_assert(sizeof(PathState) == 64 && sizeof(PathHit) == 16 && sizeof(ShadowR
 
 struct RenderParams {
     pt_camera camera;
-    int width, height, max_depth, debug, mis, brute;
+    int width, height, max_depth, debug, mis, brute, wide;
     int32_t leaves;
     const int32_t *brute_order;
 };
@@ -128,15 +128,16 @@ __global__ void extend_kernel(DeviceScene scene, RenderParams p, RenderBuffers b
     }
     const int32_t *queue = b.queue[parity];
     if (!p.brute && p.debug != PT_DEBUG_BVH && p.debug != PT_DEBUG_INTERSECTIONS) {
-        persistent_walk<false>(scene, size_t(n), &b.fetch[0], min_active, kTieLastLeaf,
-            [&](size_t k, pt_ray &r, float &lo, float &hi) { r = path_ray(b.paths[queue[k]]); lo = 0.001f; hi = FLT_MAX; },
-            [&](size_t k, const WalkResult &w) {
-                if (w.error) *b.error = 1;
-                PathHit out;
-                out.t = w.t; out.u = w.u; out.v = w.v;
-                out.slot = w.error ? -2 : w.slot;
-                b.hits[queue[k]] = out;
-            });
+        auto get = [&](size_t k, pt_ray &r, float &lo, float &hi) { r = path_ray(b.paths[queue[k]]); lo = 0.001f; hi = FLT_MAX; };
+        auto done = [&](size_t k, const WalkResult &w) {
+            if (w.error) *b.error = 1;
+            PathHit out;
+            out.t = w.t; out.u = w.u; out.v = w.v;
+            out.slot = w.error ? -2 : w.slot;
+            b.hits[queue[k]] = out;
+        };
+        if (p.wide) persistent_walk4<false>(scene, size_t(n), &b.fetch[0], min_active, kTieLastLeaf, get, done);
+        else persistent_walk<false>(scene, size_t(n), &b.fetch[0], min_active, kTieLastLeaf, get, done);
         return;
     }
     const bool reference_order = p.debug == PT_DEBUG_BVH || p.debug == PT_DEBUG_INTERSECTIONS;
@@ -301,6 +302,7 @@ __global__ void finish_kernel(DeviceScene scene, RenderParams p, RenderBuffers b
             bool hit;
             if (p.brute) hit = traverse_brute<false>(scene, p.brute_order, p.leaves, r, 0.001f, FLT_MAX, kTieLastNode, hi, prims);
             else if (reference_order) hit = traverse_reference(scene, r, 0.001f, FLT_MAX, kTieLastLeaf, hi, boxes, prims, error);
+            else if (p.wide) hit = traverse4<false>(scene, r, 0.001f, FLT_MAX, kTieLastLeaf, hi, boxes, prims, error);
             else hit = traverse<false>(scene, r, 0.001f, FLT_MAX, kTieLastLeaf, hi, boxes, prims, error);
             if (error) *b.error = 1;
             PathHit h;
@@ -318,7 +320,8 @@ __global__ void finish_kernel(DeviceScene scene, RenderParams p, RenderBuffers b
                 uint32_t sb = 0, spr = 0;
                 int serr = 0;
                 bool blocked = p.brute ? traverse_brute<true>(scene, p.brute_order, p.leaves, q, 0.001f, sr.tmax, kTieLastNode, sh, spr)
-                                       : traverse<true>(scene, q, 0.001f, sr.tmax, kTieLastLeaf, sh, sb, spr, serr);
+                             : p.wide ? traverse4<true>(scene, q, 0.001f, sr.tmax, kTieLastLeaf, sh, sb, spr, serr)
+                                      : traverse<true>(scene, q, 0.001f, sr.tmax, kTieLastLeaf, sh, sb, spr, serr);
                 if (serr) *b.error = 1;
                 else if (!blocked) { s.rr = s.rr + sr.cr; s.rg = s.rg + sr.cg; s.rb = s.rb + sr.cb; }
             }
@@ -341,18 +344,19 @@ __global__ void shadow_kernel(DeviceScene scene, RenderParams p, RenderBuffers b
         s.rr = s.rr + sr.cr; s.rg = s.rg + sr.cg; s.rb = s.rb + sr.cb;
     };
     if (!p.brute) {
-        persistent_walk<true>(scene, size_t(n), &b.fetch[1], min_active, kTieLastLeaf,
-            [&](size_t k, pt_ray &r, float &lo, float &hi) {
-                const ShadowRay &sr = b.shadows[b.shadow_queue[k]];
-                r.origin = pt_vec3{sr.ox, sr.oy, sr.oz};
-                r.direction = pt_vec3{sr.dx, sr.dy, sr.dz};
-                r.time = sr.time;
-                lo = 0.001f; hi = sr.tmax;
-            },
-            [&](size_t k, const WalkResult &w) {
-                if (w.error) { *b.error = 1; return; }
-                if (w.slot < 0) { int32_t i = b.shadow_queue[k]; add(i, b.shadows[i]); }
-            });
+        auto get = [&](size_t k, pt_ray &r, float &lo, float &hi) {
+            const ShadowRay &sr = b.shadows[b.shadow_queue[k]];
+            r.origin = pt_vec3{sr.ox, sr.oy, sr.oz};
+            r.direction = pt_vec3{sr.dx, sr.dy, sr.dz};
+            r.time = sr.time;
+            lo = 0.001f; hi = sr.tmax;
+        };
+        auto done = [&](size_t k, const WalkResult &w) {
+            if (w.error) { *b.error = 1; return; }
+            if (w.slot < 0) { int32_t i = b.shadow_queue[k]; add(i, b.shadows[i]); }
+        };
+        if (p.wide) persistent_walk4<true>(scene, size_t(n), &b.fetch[1], min_active, kTieLastLeaf, get, done);
+        else persistent_walk<true>(scene, size_t(n), &b.fetch[1], min_active, kTieLastLeaf, get, done);
         return;
     }
     for (int32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
@@ -382,7 +386,10 @@ __global__ void pack_pixels(const float *sum, unsigned char *rgba, size_t count,
     rgba[4 * i + 3] = 255;
 }
 
-size_t stack_bytes(int block) { return size_t(kSharedStack) * size_t(block) * sizeof(int32_t); }
+// shared-memory stack of the persistent walks (the larger of the two layouts' needs)
+size_t stack_bytes(int block) {
+    return std::max(size_t(kSharedStack) * sizeof(int32_t), size_t(kSharedStack4) * sizeof(int2)) * size_t(block);
+}
 
 int occupancy_grid(const void *kernel, int block, size_t smem = 0) {
     int per_sm = 0;
@@ -457,6 +464,7 @@ pt_status pt_renderer_create(const pt_scene *scene, const pt_camera *camera, int
             p.camera = *camera; p.width = width; p.height = height; p.max_depth = max_depth;
             p.debug = debug_mode; p.mis = (flags & PT_RENDER_MIS) ? 1 : 0; p.brute = (flags & PT_RENDER_BRUTE) ? 1 : 0;
             p.leaves = scene->leaf_count; p.brute_order = scene->brute_order.get<int32_t>();
+            p.wide = (g_query_config.wide && scene->view.nodes4) ? 1 : 0;
             r->paths.resize(n * sizeof(PathState));
             r->hits.resize(n * sizeof(PathHit));
             if (debug_mode == PT_DEBUG_BVH || debug_mode == PT_DEBUG_INTERSECTIONS) r->stats.resize(n * sizeof(uint2));

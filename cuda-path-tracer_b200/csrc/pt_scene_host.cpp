@@ -163,6 +163,103 @@ std::vector<pt_light> scene_lights(const pt_scene_desc &s, float &total_area) {
     return lights;
 }
 
+namespace {
+// Collapses the binary flat tree into four-wide nodes.  A child whose subtree holds at most
+// kLeafMax primitives of one type becomes a leaf over its (consecutive, depth-first) slots;
+// larger children are opened, largest surface area first, until a node has four children.
+void build_wide(const pt_scene_desc &s, const std::vector<int32_t> &slot, int32_t tri_slots, HostLayout &out) {
+    const pt_node *nodes = s.nodes;
+    const size_t n = s.node_count;
+    // subtree primitive count, type mask (1 triangle, 2 sphere) and first slot, post-order
+    std::vector<int32_t> count(n, 0), first(n, INT32_MAX);
+    std::vector<unsigned char> types(n, 0);
+    std::vector<int32_t> order;
+    order.reserve(n);
+    std::vector<std::pair<int32_t, bool>> st{{s.root, false}};
+    while(!st.empty()) {
+        auto [id, expanded] = st.back(); st.pop_back();
+        const pt_node &nd = nodes[id];
+        if(nd.type != PT_BRANCH) {
+            count[size_t(id)] = 1;
+            types[size_t(id)] = nd.type == PT_TRIANGLE ? 1 : 2;
+            first[size_t(id)] = nd.type == PT_TRIANGLE ? slot[size_t(id)] : tri_slots + slot[size_t(id)];
+            continue;
+        }
+        if(expanded) {
+            const int32_t a = nd.left, b = nd.right;
+            count[size_t(id)] = count[size_t(a)] + (b != a ? count[size_t(b)] : 0);
+            types[size_t(id)] = types[size_t(a)] | types[size_t(b)];
+            first[size_t(id)] = std::min(first[size_t(a)], first[size_t(b)]);
+            continue;
+        }
+        st.push_back({id, true});
+        st.push_back({nd.left, false});
+        if(nd.right != nd.left) st.push_back({nd.right, false});
+    }
+    auto leafable = [&](int32_t id) {
+        return count[size_t(id)] <= kLeafMax && (types[size_t(id)] == 1 || types[size_t(id)] == 2);
+    };
+    auto area = [&](int32_t id) {
+        const pt_node &nd = nodes[id];
+        double dx = double(nd.maximum.x) - nd.minimum.x, dy = double(nd.maximum.y) - nd.minimum.y, dz = double(nd.maximum.z) - nd.minimum.z;
+        return dx * dy + dy * dz + dz * dx;
+    };
+    const float inf = INFINITY;
+    struct Work { int32_t flat; int32_t index; };
+    std::vector<Work> work;
+    auto make = [&](int32_t flat) {
+        int32_t index = int32_t(out.nodes4.size());
+        out.nodes4.push_back(Bvh4Node{});
+        work.push_back({flat, index});
+        return index;
+    };
+    // the root: a single leaf cluster becomes one child of a root node
+    if(leafable(s.root)) {
+        Bvh4Node r{};
+        for(int k = 0; k < 4; k++) { r.lox[k] = r.loy[k] = r.loz[k] = inf; r.hix[k] = r.hiy[k] = r.hiz[k] = -inf; r.child[k] = kEmptyChild; }
+        const pt_node &nd = nodes[s.root];
+        r.lox[0] = nd.minimum.x; r.hix[0] = nd.maximum.x; r.loy[0] = nd.minimum.y; r.hiy[0] = nd.maximum.y;
+        r.loz[0] = nd.minimum.z; r.hiz[0] = nd.maximum.z;
+        r.child[0] = ~((first[size_t(s.root)] << 3) | (count[size_t(s.root)] - 1));
+        out.nodes4.push_back(r);
+        return;
+    }
+    if(size_t(tri_slots) + s.sphere_count >= (size_t(1) << 28)) { out.nodes4.clear(); return; }
+    make(s.root);
+    while(!work.empty()) {
+        Work w = work.back(); work.pop_back();
+        std::vector<int32_t> kids;
+        const pt_node &nd = nodes[w.flat];
+        kids.push_back(nd.left);
+        if(nd.right != nd.left) kids.push_back(nd.right);
+        while(kids.size() < 4) {
+            int best = -1;
+            double best_area = -1;
+            for(size_t k = 0; k < kids.size(); k++) {
+                const pt_node &c = nodes[kids[k]];
+                if(c.type != PT_BRANCH || leafable(kids[k])) continue;
+                double a = area(kids[k]);
+                if(a > best_area) { best_area = a; best = int(k); }
+            }
+            if(best < 0) break;
+            const pt_node &c = nodes[kids[size_t(best)]];
+            kids[size_t(best)] = c.left;
+            if(c.right != c.left) kids.insert(kids.begin() + best + 1, c.right);
+        }
+        Bvh4Node r{};
+        for(int k = 0; k < 4; k++) { r.lox[k] = r.loy[k] = r.loz[k] = inf; r.hix[k] = r.hiy[k] = r.hiz[k] = -inf; r.child[k] = kEmptyChild; }
+        for(size_t k = 0; k < kids.size(); k++) {
+            const pt_node &c = nodes[kids[k]];
+            r.lox[k] = c.minimum.x; r.hix[k] = c.maximum.x; r.loy[k] = c.minimum.y; r.hiy[k] = c.maximum.y;
+            r.loz[k] = c.minimum.z; r.hiz[k] = c.maximum.z;
+            if(leafable(kids[k])) r.child[k] = ~((first[size_t(kids[k])] << 3) | (count[size_t(kids[k])] - 1));
+            else r.child[k] = make(kids[k]);
+        }
+        out.nodes4[size_t(w.index)] = r;
+    }
+}
+} // namespace
+
 // Re-layout: one 64-byte node per flat branch (reachable from the root), holding both
 // children's boxes; leaves become slots into the 48-byte triangle / 32-byte sphere arrays,
 // numbered in first-visit depth-first order so a subtree's leaves are contiguous.
@@ -255,6 +352,18 @@ HostLayout relayout(const pt_scene_desc &s) {
         r.cx = p.center.x; r.cy = p.center.y; r.cz = p.center.z; r.radius = p.radius;
         r.id = id; r.node = sphere_leaves[k];
         out.spheres[k] = r;
+    }
+    // Four-wide collapse (trees only: a node reached twice keeps the two-wide layout).
+    {
+        std::vector<int32_t> parents(s.node_count, 0);
+        bool shared = false;
+        for(size_t id = 0; id < s.node_count && !shared; id++) {
+            if(inner[id] < 0) continue;
+            const pt_node &p = nodes[id];
+            if(++parents[size_t(p.left)] > 1) shared = true;
+            if(p.right != p.left && ++parents[size_t(p.right)] > 1) shared = true;
+        }
+        if(!shared) build_wide(s, slot, tri_slots, out);
     }
     // brute order: leaves in flat node-array order
     for(size_t id = 0; id < s.node_count; id++) {

@@ -492,3 +492,209 @@ __device__ inline void persistent_walk(const DeviceScene &s, size_t count, unsig
 
 } // namespace ptb
 #endif
+
+namespace ptb {
+
+// ---- four-wide traversal -------------------------------------------------------------------
+// Same answer as traverse<> (same primitive tests, same limit rule, same tie keys); fewer,
+// wider steps.  A step tests the four child boxes of a node with the reference's slab
+// arithmetic, visits the nearest passing child next and pushes the others, farthest first,
+// with their entry distance; a popped entry whose entry distance is no longer below the
+// current limit is dropped, which is exactly the box test repeated with the new limit.
+
+PT_HD inline void load_node4(const DeviceScene &s, int32_t node, Bvh4Node &n) {
+#ifdef __CUDA_ARCH__
+    const float4 *p = reinterpret_cast<const float4 *>(&s.nodes4[node]);
+    float4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2), d = __ldg(p + 3), e = __ldg(p + 4), f = __ldg(p + 5);
+    int4 g = __ldg(reinterpret_cast<const int4 *>(p + 6));
+    n.lox[0] = a.x; n.lox[1] = a.y; n.lox[2] = a.z; n.lox[3] = a.w;
+    n.hix[0] = b.x; n.hix[1] = b.y; n.hix[2] = b.z; n.hix[3] = b.w;
+    n.loy[0] = c.x; n.loy[1] = c.y; n.loy[2] = c.z; n.loy[3] = c.w;
+    n.hiy[0] = d.x; n.hiy[1] = d.y; n.hiy[2] = d.z; n.hiy[3] = d.w;
+    n.loz[0] = e.x; n.loz[1] = e.y; n.loz[2] = e.z; n.loz[3] = e.w;
+    n.hiz[0] = f.x; n.hiz[1] = f.y; n.hiz[2] = f.z; n.hiz[3] = f.w;
+    n.child[0] = g.x; n.child[1] = g.y; n.child[2] = g.z; n.child[3] = g.w;
+#else
+    n = s.nodes4[node];
+#endif
+}
+
+// Tests the children of `node`; returns how many passed, in `ref`/`dist` sorted nearest first.
+PT_HD inline int node4_children(const DeviceScene &s, int32_t node, const RayBox &rb, float tmin, float limit,
+                                int32_t ref[4], float dist[4], uint32_t &boxes) {
+    Bvh4Node n;
+    load_node4(s, node, n);
+    int hits = 0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        float e;
+        bool h = n.child[k] != kEmptyChild && box_hit(rb, n.lox[k], n.hix[k], n.loy[k], n.hiy[k], n.loz[k], n.hiz[k], tmin, limit, e);
+        boxes += n.child[k] != kEmptyChild;
+        ref[k] = n.child[k];
+        dist[k] = h ? e : INFINITY;
+        hits += h;
+    }
+    // sorting network on (dist, ref), ascending
+#define PT_CSWAP(i, j) if (dist[j] < dist[i]) { float td = dist[i]; dist[i] = dist[j]; dist[j] = td; int32_t tr = ref[i]; ref[i] = ref[j]; ref[j] = tr; }
+    PT_CSWAP(0, 1) PT_CSWAP(2, 3) PT_CSWAP(0, 2) PT_CSWAP(1, 3) PT_CSWAP(1, 2)
+#undef PT_CSWAP
+    return hits;
+}
+
+// Tests the 1..8 slots of a leaf reference; true when kAny and a hit was found.
+template <bool kAny>
+PT_HD inline bool leaf4(const DeviceScene &s, int32_t ref, const pt_ray &r, float dl, float tmin, float tmax, int tie,
+                        bool &found, float &closest, long long &best_key, HitInfo &hit, uint32_t &prims) {
+    int32_t v = ~ref;
+    int32_t first = v >> 3, count = (v & 7) + 1;
+    for (int32_t j = 0; j < count; j++)
+        if (test_leaf<kAny>(s, first + j, r, dl, tmin, tmax, tie, found, closest, best_key, hit, prims) && kAny) return true;
+    return false;
+}
+
+// Per-thread four-wide walk (local-memory stack), for kernels that run one ray per thread.
+template <bool kAny>
+PT_HD inline bool traverse4(const DeviceScene &s, const pt_ray &r, float tmin, float tmax, int tie,
+                            HitInfo &hit, uint32_t &boxes, uint32_t &prims, int &error) {
+    hit.slot = -1; hit.t = 0; hit.u = 0; hit.v = 0;
+    if (s.empty || s.node_count == 0) return false;
+    RayBox rb = ray_box(r);
+    float dl = length(mk(r.direction));
+    bool found = false;
+    float closest = tmax, limit = tmax;
+    long long best_key = 0;
+    int32_t sref[3 * kStackCapacity];
+    float sdist[3 * kStackCapacity];
+    int sp = 0;
+    int32_t cur = 0;   // root node
+    for (;;) {
+        if (cur >= 0) {
+            int32_t ref[4];
+            float dist[4];
+            int hits = node4_children(s, cur, rb, tmin, limit, ref, dist, boxes);
+            if (hits) {
+                if (sp + hits - 1 > 3 * kStackCapacity) { error = 1; hit.slot = -1; return false; }
+                for (int k = hits - 1; k >= 1; k--) { sref[sp] = ref[k]; sdist[sp] = dist[k]; sp++; }
+                cur = ref[0];
+                continue;
+            }
+        } else {
+            if (leaf4<kAny>(s, cur, r, dl, tmin, tmax, tie, found, closest, best_key, hit, prims) && kAny) return true;
+            if (found) limit = nextafterf(closest, tmax);
+        }
+        // pop the nearest entry still inside the limit
+        bool next = false;
+        while (sp > 0) {
+            sp--;
+            if (sdist[sp] < limit) { cur = sref[sp]; next = true; break; }
+        }
+        if (!next) break;
+    }
+    return found;
+}
+
+} // namespace ptb
+
+#ifdef __CUDACC__
+namespace ptb {
+
+// Four-wide form of persistent_walk (same contract).  Each lane keeps kSharedStack4 stack
+// entries (reference + entry distance) in shared memory, entry-major, the rest in local memory.
+constexpr int kSharedStack4 = 16;
+constexpr int kStack4 = 3 * kStackCapacity;
+
+template <bool kAny, class Get, class Done>
+__device__ inline void persistent_walk4(const DeviceScene &s, size_t count, unsigned long long *next, int min_active,
+                                        int tie, Get get, Done done) {
+    const size_t warp_first = (size_t(blockIdx.x) * blockDim.x + (threadIdx.x & ~31u));
+    if (warp_first >= count) return;
+    extern __shared__ int32_t shared_stack[];
+    int2 *my_stack = reinterpret_cast<int2 *>(shared_stack) + threadIdx.x;
+    const int stride = blockDim.x;
+    int2 spill[kStack4 - kSharedStack4];
+    const unsigned lane = threadIdx.x & 31;
+    pt_ray r;
+    RayBox rb;
+    float dl = 0, tmin = 0, tmax = 0, closest = 0, limit = 0;
+    long long best_key = 0;
+    HitInfo hit;
+    uint32_t boxes = 0, prims = 0;
+    int32_t cur = -1;
+    int sp = 0;
+    bool found = false;
+    int error = 0;
+    size_t index = 0;
+    bool busy = false, pool_empty = false;
+    hit.slot = -1; hit.t = 0; hit.u = 0; hit.v = 0;
+    for (;;) {
+        unsigned idle = __ballot_sync(0xffffffffu, !busy);
+        if (idle && !pool_empty) {
+            int leader = __ffs(idle) - 1;
+            unsigned long long base = 0;
+            if ((int)lane == leader) base = atomicAdd(next, (unsigned long long)__popc(idle));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (base + __popc(idle) >= count) pool_empty = true;
+            if (!busy) {
+                size_t mine = base + __popc(idle & ((1u << lane) - 1u));
+                if (mine < count) {
+                    index = mine;
+                    get(index, r, tmin, tmax);
+                    rb = ray_box(r);
+                    dl = length(mk(r.direction));
+                    closest = tmax; limit = tmax; best_key = 0;
+                    hit.slot = -1; hit.t = 0; hit.u = 0; hit.v = 0;
+                    boxes = 0; prims = 0; sp = 0; found = false; error = 0;
+                    cur = (s.empty || s.node_count == 0) ? kEmptyChild : 0;
+                    busy = true;
+                }
+            }
+        }
+        if (!__any_sync(0xffffffffu, busy)) break;
+        const int threshold = pool_empty ? 1 : min_active;
+        for (;;) {
+            if (busy) {
+                bool end = cur == kEmptyChild, descended = false;
+                if (!end && cur >= 0) {
+                    int32_t ref[4];
+                    float dist[4];
+                    int hits = node4_children(s, cur, rb, tmin, limit, ref, dist, boxes);
+                    if (hits) {
+                        if (sp + hits - 1 > kStack4) { error = 1; found = false; end = true; }
+                        else {
+                            for (int k = hits - 1; k >= 1; k--) {
+                                int2 e = make_int2(ref[k], __float_as_int(dist[k]));
+                                if (sp < kSharedStack4) my_stack[sp * stride] = e; else spill[sp - kSharedStack4] = e;
+                                sp++;
+                            }
+                            cur = ref[0];
+                            descended = true;
+                        }
+                    }
+                } else if (!end) {
+                    if (leaf4<kAny>(s, cur, r, dl, tmin, tmax, tie, found, closest, best_key, hit, prims) && kAny) end = true;
+                    else if (found) limit = nextafterf(closest, tmax);
+                }
+                if (!end && !descended) {
+                    end = true;
+                    while (sp > 0) {
+                        sp--;
+                        int2 e = sp < kSharedStack4 ? my_stack[sp * stride] : spill[sp - kSharedStack4];
+                        if (__int_as_float(e.y) < limit) { cur = e.x; end = false; break; }
+                    }
+                }
+                if (end) {
+                    WalkResult res;
+                    res.t = hit.t; res.u = hit.u; res.v = hit.v; res.slot = found ? hit.slot : -1;
+                    res.boxes = boxes; res.prims = prims; res.error = error;
+                    done(index, res);
+                    busy = false;
+                    cur = kEmptyChild;
+                }
+            }
+            if (__popc(__ballot_sync(0xffffffffu, busy)) < threshold) break;
+        }
+    }
+}
+
+} // namespace ptb
+#endif

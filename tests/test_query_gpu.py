@@ -30,6 +30,14 @@ def oracle():
     return Oracle()
 
 
+@pytest.fixture(params=[1, 0], ids=["wide", "binary"])
+def layout(request):
+    """Runs a test with the four-wide and with the two-wide node layout."""
+    pt.query_layout(request.param)
+    yield request.param
+    pt.query_layout(1)
+
+
 def assert_hits_equal(got, want):
     assert got.dtype == pt.HIT and want.dtype == pt.HIT
     assert np.array_equal(got["primitive_type"], want["primitive_type"])
@@ -56,21 +64,21 @@ def assert_trace_results(got, want):
 
 
 @pytest.mark.parametrize("brute", [False, True])
-def test_compat_matches_reference_golden(brute):
+def test_compat_matches_reference_golden(brute, layout):
     """cuda_query_rays semantics: full 56-byte trace_result, reference tie rule."""
     s = golden_scene("cornell")
     got = pt.cuda_query_rays(s, G["cornell_rays"], brute=brute)
     assert_trace_results(got, G[f"cornell_result_brute{int(brute)}"])
 
 
-def test_compat_reference_pipeline_scene():
+def test_compat_reference_pipeline_scene(layout):
     s = golden_scene("sphere")
     got = pt.cuda_query_rays(s, G["sphere_rays"])
     assert_trace_results(got, G["sphere_result"])
 
 
 @pytest.mark.parametrize("prefix", ["cornell", "sphere", "light0", "light1"])
-def test_closest_and_any_vs_oracle(oracle, prefix):
+def test_closest_and_any_vs_oracle(oracle, prefix, layout):
     s = golden_scene(prefix)
     rays = G["cornell_rays"] if prefix == "cornell" else G["sphere_rays"] if prefix == "sphere" else \
         pt.camera_rays(G[f"{prefix}_camera"], 19, 13, 5, 0, 2048)
@@ -81,7 +89,7 @@ def test_closest_and_any_vs_oracle(oracle, prefix):
     assert np.array_equal(got_any["primitive_type"] != 0, want_any["primitive_id"] >= 0)
 
 
-def test_tmax_and_stats(oracle):
+def test_tmax_and_stats(oracle, layout):
     s = golden_scene("cornell")
     rays, tmax = G["cornell_rays"], G["cornell_tmax"]
     dev = pt.Scene(s)
@@ -90,7 +98,7 @@ def test_tmax_and_stats(oracle):
     assert (stats["primitives"] >= (hits["primitive_type"] != 0)).all()
 
 
-def test_exact_tie_lowest_id():
+def test_exact_tie_lowest_id(layout):
     """transport_tests' pruning scene (tests/transport_tests.cpp:54-78): two coincident spheres.
     The reference keeps the later leaf (material 1); the north-star rule keeps the lowest id."""
     spheres = np.zeros(3, pt.SPHERE)
@@ -116,7 +124,7 @@ def test_exact_tie_lowest_id():
     assert hits["primitive_id"][0] == 0 and hits["primitive_type"][0] == pt.SPHERE_TYPE and hits["t"][0] == 2.0
 
 
-def test_empty_and_single_primitive_scenes(oracle):
+def test_empty_and_single_primitive_scenes(oracle, layout):
     empty = pt.FlatScene()
     rays = G["cornell_rays"][:64]
     hits = pt.Scene(empty).query(rays)
@@ -137,7 +145,7 @@ def test_empty_and_single_primitive_scenes(oracle):
     assert_hits_equal(got, oracle.query(one, r, tmin=0.0))
 
 
-def test_brute_device_equals_bvh(oracle):
+def test_brute_device_equals_bvh(oracle, layout):
     s, cam = pt.cornell_box(64, 40)
     dev = pt.Scene(s)
     torch = pytest.importorskip("torch")
@@ -151,7 +159,7 @@ def test_brute_device_equals_bvh(oracle):
     assert torch.equal(a, b)
 
 
-def test_procedural_scene_vs_oracle(oracle):
+def test_procedural_scene_vs_oracle(oracle, layout):
     """A 4-sphere, 64k-triangle displaced-sphere scene: camera rays and bounce rays."""
     torch = pytest.importorskip("torch")
     s, cam = pt.procedural_scene(96, 60, sphere_count=4, segments=128, rings=65, seed=3)
@@ -179,7 +187,7 @@ def test_procedural_scene_vs_oracle(oracle):
 
 
 @pytest.mark.skipif(not REF_GPU_SO.exists(), reason="reference CUDA build absent")
-def test_matches_reference_gpu_query():
+def test_matches_reference_gpu_query(layout):
     """Our compatibility query and the reference's own cuda_query_rays on the same B200."""
     s = golden_scene("cornell")
     want = RefGpu().query(s, G["cornell_rays"])

@@ -173,8 +173,11 @@ def test_bit_identical_to_reference_gpu_renderer(debug):
 
 @pytest.mark.skipif(not REF_GPU_SO.exists(), reason="reference CUDA build absent")
 @pytest.mark.parametrize("tail", [0, None, 2**31 - 1], ids=["wavefront", "hybrid", "fused"])
-def test_bit_identical_to_reference_gpu_cornell(tail):
-    """Pure wavefront, the default hybrid and the fused finish kernel all give the reference's bits."""
+@pytest.mark.parametrize("wide", [1, 0], ids=["wide", "binary"])
+def test_bit_identical_to_reference_gpu_cornell(tail, wide):
+    """Pure wavefront, the default hybrid and the fused finish kernel, on either node layout, all
+    give the reference's bits."""
+    pt.query_layout(wide)
     s, cam = pt.cornell_box(64, 40)
     ref = RefGpu().renderer(s, cam, 64, 40, 1)
     ref.add_samples(4)
@@ -182,6 +185,7 @@ def test_bit_identical_to_reference_gpu_cornell(tail):
     if tail is not None:
         ours.set_tail_paths(tail)
     ours.add_samples(4)
+    pt.query_layout(1)
     assert ours.image().tobytes() == ref.image().tobytes()
     assert ours.rays_traced() == ref.stats()[2]
     ref.close()
