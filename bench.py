@@ -121,12 +121,17 @@ def reference_rays(scene, cam, count_each: int, ref):
     return np.concatenate([prim, bounce])
 
 
-def cpu_reference_rate(scene, rays, ref, threads: int):
-    """Reference trace_world over `rays` on `threads` host threads: (rays/s, seconds, stats)."""
+def cpu_reference_rate(scene, rays, ref, threads: int, chunk: int = 1 << 20):
+    """Reference trace_world over `rays` on `threads` host threads, in chunks (bounded memory):
+    (rays/s, seconds, per-ray mean box tests, per-ray mean primitive tests)."""
+    boxes = prims = 0.0
     t = time.perf_counter()
-    _, stats = ref.trace_world(scene, rays, nthreads=threads)
+    for b in range(0, len(rays), chunk):
+        _, stats = ref.trace_world(scene, rays[b:b + chunk], nthreads=threads)
+        boxes += float(stats["boxes"].sum())
+        prims += float(stats["primitives"].sum())
     dt = time.perf_counter() - t
-    return len(rays) / dt, dt, stats
+    return len(rays) / dt, dt, boxes / len(rays), prims / len(rays)
 
 
 def run_reference(args):
@@ -138,7 +143,7 @@ def run_reference(args):
     ref = RefCpu()
     threads = os.cpu_count() or 1
     scene, cam, _ = build_scene()
-    per = 1 << 16
+    per = 1 << 18
     sample = reference_rays(scene, cam, per, ref)
     for _ in range(args.warmup):
         cpu_reference_rate(scene, sample, ref, threads)
@@ -151,7 +156,7 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "sample": f"{len(sample)} rays per step (first 2^16 camera + their bounce rays)"},
+        "config": {"workload": WORKLOAD, "sample": f"{len(sample)} rays per step (first {per} camera rays + their bounce rays)"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
                          "sample": f"{len(sample)} rays per step, trace_world on host_view"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -265,15 +270,14 @@ def main():
         if REF_CPU_SO.exists():
             ref = RefCpu()
             threads = os.cpu_count() or 1
-            per = 1 << 15
+            # grow the sample until it holds ~10 s of traversal on all host cores (cap 2^23 + 2^23 rays)
+            per = 1 << 16
             sample = reference_rays(scene, cam, per, ref)
-            rate, dt, rstats = cpu_reference_rate(scene, sample, ref, threads)
-            while dt < 3.0 and per < (1 << 20):
-                per *= 4
+            rate, dt, n_box, n_tri = cpu_reference_rate(scene, sample, ref, threads)
+            while dt < 10.0 and per < (1 << 23):
+                per = min(1 << 23, per * max(2, 1 << int(np.log2(max(1.0, 10.0 / max(dt, 1e-3))))))
                 sample = reference_rays(scene, cam, per, ref)
-                rate, dt, rstats = cpu_reference_rate(scene, sample, ref, threads)
-            n_box = float(rstats["boxes"].mean())
-            n_tri = float(rstats["primitives"].mean())
+                rate, dt, n_box, n_tri = cpu_reference_rate(scene, sample, ref, threads)
             cpu = {"value": rate / 1e9, "unit": UNIT, "cores": threads, "kind": "reference",
                    "sample": f"{len(sample)} rays (first {per} camera rays + their bounce rays), "
                              f"trace_world on host_view, {dt:.2f} s"}

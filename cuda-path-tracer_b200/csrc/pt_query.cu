@@ -55,7 +55,7 @@ __global__ void __launch_bounds__(kQueryBlock) query_kernel(DeviceScene s, const
 // Persistent form: a fixed grid of warps; each warp takes rays from a global counter and,
 // between traversal steps, hands a new ray to every lane whose ray has ended once fewer than
 // `min_active` lanes are still busy.  next_ray must be zero at launch.
-template <bool kAny, bool kStats, bool kWide>
+template <bool kAny, bool kStats, int kWalk>
 __global__ void __launch_bounds__(kQueryBlock) query_persistent_kernel(DeviceScene s, const pt_ray *__restrict__ rays, size_t count,
                                                                        float tmin, const float *__restrict__ tmax,
                                                                        pt_hit *__restrict__ hits, pt_ray_stats *__restrict__ stats,
@@ -68,7 +68,8 @@ __global__ void __launch_bounds__(kQueryBlock) query_persistent_kernel(DeviceSce
         reinterpret_cast<int4 *>(hits)[k] = make_int4(__float_as_int(hit ? w.t : 0.0f), id, type, w.error);
         if (kStats) { stats[k].boxes = w.boxes; stats[k].primitives = w.prims; }
     };
-    if (kWide) persistent_walk4<kAny>(s, count, next_ray, min_active, tie, get, done);
+    if (kWalk == 2) persistent_walk4_spec<kAny>(s, count, next_ray, min_active, tie, get, done);
+    else if (kWalk == 1) persistent_walk4<kAny>(s, count, next_ray, min_active, tie, get, done);
     else persistent_walk<kAny>(s, count, next_ray, min_active, tie, get, done);
 }
 
@@ -156,14 +157,15 @@ void launch_query(const pt_scene *sc, const pt_ray *rays, size_t count, int mode
         const bool any = mode == PT_QUERY_ANY;
         using Fn = void (*)(DeviceScene, const pt_ray *, size_t, float, const float *, pt_hit *, pt_ray_stats *, int,
                             unsigned long long *, int);
-        static const Fn table[8] = {
-            query_persistent_kernel<false, false, false>, query_persistent_kernel<false, false, true>,
-            query_persistent_kernel<false, true, false>, query_persistent_kernel<false, true, true>,
-            query_persistent_kernel<true, false, false>, query_persistent_kernel<true, false, true>,
-            query_persistent_kernel<true, true, false>, query_persistent_kernel<true, true, true>};
-        int k = (any ? 4 : 0) + (stats ? 2 : 0) + (wide ? 1 : 0);
+        static const Fn table[12] = {
+            query_persistent_kernel<false, false, 0>, query_persistent_kernel<false, false, 1>, query_persistent_kernel<false, false, 2>,
+            query_persistent_kernel<false, true, 0>, query_persistent_kernel<false, true, 1>, query_persistent_kernel<false, true, 2>,
+            query_persistent_kernel<true, false, 0>, query_persistent_kernel<true, false, 1>, query_persistent_kernel<true, false, 2>,
+            query_persistent_kernel<true, true, 0>, query_persistent_kernel<true, true, 1>, query_persistent_kernel<true, true, 2>};
+        int walk = wide ? (g_query_config.speculative ? 2 : 1) : 0;
+        int k = (any ? 6 : 0) + (stats ? 3 : 0) + walk;
         Fn fn = table[k];
-        static int per_sm[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        static int per_sm[12] = {0};
         const size_t smem = wide ? size_t(kSharedStack4) * kQueryBlock * sizeof(int2) : size_t(kSharedStack) * kQueryBlock * sizeof(int32_t);
         if(!per_sm[k]) PT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[k], (const void *)fn, kQueryBlock, smem));
         int bps = g_query_config.blocks_per_sm > 0 ? std::min(g_query_config.blocks_per_sm, per_sm[k]) : per_sm[k];
@@ -382,6 +384,11 @@ pt_status pt_query_tuning(int persistent, int min_active, int blocks_per_sm) {
 // Node layout of the traversal kernels: 1 = four-wide nodes where the scene has them, 0 = two-wide.
 pt_status pt_query_layout(int wide) {
     return guard([&]() { g_query_config.wide = wide ? 1 : 0; });
+}
+
+// Four-wide walk form: 1 = node and leaf phases (speculative while-while), 0 = one loop.
+pt_status pt_query_walk(int speculative) {
+    return guard([&]() { g_query_config.speculative = speculative ? 1 : 0; });
 }
 
 pt_status pt_rays_camera_device(const pt_camera *camera, int width, int height, uint64_t seed, uint64_t first,

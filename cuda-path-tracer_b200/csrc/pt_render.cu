@@ -136,7 +136,8 @@ __global__ void extend_kernel(DeviceScene scene, RenderParams p, RenderBuffers b
             out.slot = w.error ? -2 : w.slot;
             b.hits[queue[k]] = out;
         };
-        if (p.wide) persistent_walk4<false>(scene, size_t(n), &b.fetch[0], min_active, kTieLastLeaf, get, done);
+        if (p.wide == 2) persistent_walk4_spec<false>(scene, size_t(n), &b.fetch[0], min_active, kTieLastLeaf, get, done);
+        else if (p.wide) persistent_walk4<false>(scene, size_t(n), &b.fetch[0], min_active, kTieLastLeaf, get, done);
         else persistent_walk<false>(scene, size_t(n), &b.fetch[0], min_active, kTieLastLeaf, get, done);
         return;
     }
@@ -355,7 +356,8 @@ __global__ void shadow_kernel(DeviceScene scene, RenderParams p, RenderBuffers b
             if (w.error) { *b.error = 1; return; }
             if (w.slot < 0) { int32_t i = b.shadow_queue[k]; add(i, b.shadows[i]); }
         };
-        if (p.wide) persistent_walk4<true>(scene, size_t(n), &b.fetch[1], min_active, kTieLastLeaf, get, done);
+        if (p.wide == 2) persistent_walk4_spec<true>(scene, size_t(n), &b.fetch[1], min_active, kTieLastLeaf, get, done);
+        else if (p.wide) persistent_walk4<true>(scene, size_t(n), &b.fetch[1], min_active, kTieLastLeaf, get, done);
         else persistent_walk<true>(scene, size_t(n), &b.fetch[1], min_active, kTieLastLeaf, get, done);
         return;
     }
@@ -464,7 +466,7 @@ pt_status pt_renderer_create(const pt_scene *scene, const pt_camera *camera, int
             p.camera = *camera; p.width = width; p.height = height; p.max_depth = max_depth;
             p.debug = debug_mode; p.mis = (flags & PT_RENDER_MIS) ? 1 : 0; p.brute = (flags & PT_RENDER_BRUTE) ? 1 : 0;
             p.leaves = scene->leaf_count; p.brute_order = scene->brute_order.get<int32_t>();
-            p.wide = (g_query_config.wide && scene->view.nodes4) ? 1 : 0;
+            p.wide = (g_query_config.wide && scene->view.nodes4) ? (g_query_config.speculative ? 2 : 1) : 0;
             r->paths.resize(n * sizeof(PathState));
             r->hits.resize(n * sizeof(PathHit));
             if (debug_mode == PT_DEBUG_BVH || debug_mode == PT_DEBUG_INTERSECTIONS) r->stats.resize(n * sizeof(uint2));

@@ -698,3 +698,118 @@ __device__ inline void persistent_walk4(const DeviceScene &s, size_t count, unsi
 
 } // namespace ptb
 #endif
+
+#ifdef __CUDACC__
+namespace ptb {
+
+// Four-wide walk in two phases per round (speculative while-while): in the node phase every
+// lane walks inner nodes until it holds one postponed leaf — lanes that already hold one keep
+// walking speculatively while others search — and in the leaf phase all lanes test their leaf
+// together, so node work and primitive work do not diverge inside one warp instruction
+// stream.  Same contract and answer as persistent_walk4.
+template <bool kAny, class Get, class Done>
+__device__ inline void persistent_walk4_spec(const DeviceScene &s, size_t count, unsigned long long *next, int min_active,
+                                             int tie, Get get, Done done) {
+    const size_t warp_first = (size_t(blockIdx.x) * blockDim.x + (threadIdx.x & ~31u));
+    if (warp_first >= count) return;
+    extern __shared__ int32_t shared_stack[];
+    int2 *my_stack = reinterpret_cast<int2 *>(shared_stack) + threadIdx.x;
+    const int stride = blockDim.x;
+    int2 spill[kStack4 - kSharedStack4];
+    const unsigned lane = threadIdx.x & 31;
+    constexpr int32_t kNone = kEmptyChild;
+    pt_ray r;
+    RayBox rb;
+    float dl = 0, tmin = 0, tmax = 0, closest = 0, limit = 0;
+    long long best_key = 0;
+    HitInfo hit;
+    uint32_t boxes = 0, prims = 0;
+    int32_t cur = kNone, leaf = kNone;
+    int sp = 0;
+    bool found = false;
+    int error = 0;
+    size_t index = 0;
+    bool busy = false, pool_empty = false;
+    hit.slot = -1; hit.t = 0; hit.u = 0; hit.v = 0;
+    auto pop = [&]() -> int32_t {
+        while (sp > 0) {
+            sp--;
+            int2 e = sp < kSharedStack4 ? my_stack[sp * stride] : spill[sp - kSharedStack4];
+            if (__int_as_float(e.y) < limit) return e.x;
+        }
+        return kNone;
+    };
+    for (;;) {
+        unsigned idle = __ballot_sync(0xffffffffu, !busy);
+        if (idle && !pool_empty) {
+            int leader = __ffs(idle) - 1;
+            unsigned long long base = 0;
+            if ((int)lane == leader) base = atomicAdd(next, (unsigned long long)__popc(idle));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (base + __popc(idle) >= count) pool_empty = true;
+            if (!busy) {
+                size_t mine = base + __popc(idle & ((1u << lane) - 1u));
+                if (mine < count) {
+                    index = mine;
+                    get(index, r, tmin, tmax);
+                    rb = ray_box(r);
+                    dl = length(mk(r.direction));
+                    closest = tmax; limit = tmax; best_key = 0;
+                    hit.slot = -1; hit.t = 0; hit.u = 0; hit.v = 0;
+                    boxes = 0; prims = 0; sp = 0; found = false; error = 0;
+                    cur = (s.empty || s.node_count == 0) ? kNone : 0;
+                    leaf = kNone;
+                    busy = true;
+                }
+            }
+        }
+        if (!__any_sync(0xffffffffu, busy)) break;
+        const int threshold = pool_empty ? 1 : min_active;
+        for (;;) {
+            bool end = false;
+            // ---- node phase
+            for (;;) {
+                if (busy && leaf == kNone && cur < 0) { leaf = cur; cur = pop(); }
+                bool searching = busy && leaf == kNone && cur != kNone;
+                if (!__any_sync(0xffffffffu, searching)) break;
+                if (busy && cur >= 0 && cur != kNone && !error) {
+                    int32_t ref[4];
+                    float dist[4];
+                    int hits = node4_children(s, cur, rb, tmin, limit, ref, dist, boxes);
+                    if (hits) {
+                        if (sp + hits - 1 > kStack4) { error = 1; cur = kNone; leaf = kNone; }
+                        else {
+                            for (int k = hits - 1; k >= 1; k--) {
+                                int2 e = make_int2(ref[k], __float_as_int(dist[k]));
+                                if (sp < kSharedStack4) my_stack[sp * stride] = e; else spill[sp - kSharedStack4] = e;
+                                sp++;
+                            }
+                            cur = ref[0];
+                        }
+                    } else {
+                        cur = pop();
+                    }
+                }
+            }
+            // ---- leaf phase
+            if (busy && leaf != kNone) {
+                if (leaf4<kAny>(s, leaf, r, dl, tmin, tmax, tie, found, closest, best_key, hit, prims) && kAny) end = true;
+                else if (found) limit = nextafterf(closest, tmax);
+                leaf = kNone;
+            }
+            if (busy && (end || error || (leaf == kNone && cur == kNone))) {
+                WalkResult res;
+                if (error) found = false;
+                res.t = hit.t; res.u = hit.u; res.v = hit.v; res.slot = found ? hit.slot : -1;
+                res.boxes = boxes; res.prims = prims; res.error = error;
+                done(index, res);
+                busy = false;
+                cur = kNone; leaf = kNone;
+            }
+            if (__popc(__ballot_sync(0xffffffffu, busy)) < threshold) break;
+        }
+    }
+}
+
+} // namespace ptb
+#endif

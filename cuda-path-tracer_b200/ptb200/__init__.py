@@ -115,6 +115,7 @@ def library() -> C.CDLL:
         "pt_query_rays_compat": (I, [P, P, S, I, P]),
         "pt_query_tuning": (I, [I, I, I]),
         "pt_query_layout": (I, [I]),
+        "pt_query_walk": (I, [I]),
         "pt_rays_camera_device": (I, [P, I, I, U64, U64, S, P, P]),
         "pt_rays_bounce_device": (I, [P, P, P, S, U64, U64, P, P]),
         "pt_flat_from_desc": (I, [P, P]),
@@ -393,7 +394,7 @@ def camera_rays_device(camera: np.ndarray, width, height, seed, first, count, ou
     check(library().pt_rays_camera_device(camera.ctypes.data, width, height, seed, first, count, _ptr(out), stream))
 
 
-def query_tuning(persistent: int = 1, min_active: int = 24, blocks_per_sm: int = 0) -> None:
+def query_tuning(persistent: int = 1, min_active: int = 16, blocks_per_sm: int = 0) -> None:
     """Sets the ray-query kernel variant and its tunables (pt_query_tuning)."""
     check(library().pt_query_tuning(persistent, min_active, blocks_per_sm))
 
@@ -401,6 +402,11 @@ def query_tuning(persistent: int = 1, min_active: int = 24, blocks_per_sm: int =
 def query_layout(wide: int = 1) -> None:
     """Four-wide (1) or two-wide (0) node layout for the traversal kernels (pt_query_layout)."""
     check(library().pt_query_layout(int(wide)))
+
+
+def query_walk(speculative: int = 1) -> None:
+    """Four-wide walk form: node/leaf phases (1) or a single loop (0) (pt_query_walk)."""
+    check(library().pt_query_walk(int(speculative)))
 
 
 def cuda_query_rays(scene: FlatScene, rays: np.ndarray, brute: bool = False) -> np.ndarray:

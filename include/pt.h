@@ -148,12 +148,15 @@ pt_status pt_query_rays_brute_device(const pt_scene *scene, const pt_ray *rays, 
 /* Tuning of the ray-query kernel (process-wide): persistent = 1 runs a fixed grid of warps that
  * take rays from a global counter and refill lanes whose ray has ended once fewer than
  * `min_active` (1..32) lanes are busy; persistent = 0 launches one thread per ray.
- * blocks_per_sm = 0 uses the occupancy limit.  Defaults: 1, 24, 0. */
+ * blocks_per_sm = 0 uses the occupancy limit.  Defaults: 1, 16, 0. */
 pt_status pt_query_tuning(int persistent, int min_active, int blocks_per_sm);
 /* Node layout of the traversal kernels (process-wide; renderers pick it up when created):
  * 1 = four-wide nodes (up to 4 primitives per leaf) where the scene's tree allows it (default),
  * 0 = the two-wide re-layout of the caller's tree.  Results do not depend on it. */
 pt_status pt_query_layout(int wide);
+/* Four-wide walk form (process-wide): 1 = separate node and leaf phases per warp round, lanes
+ * that already hold a leaf walking on speculatively (default); 0 = nodes and leaves in one loop. */
+pt_status pt_query_walk(int speculative);
 
 /* ---- device ray generators (bit-identical to the host ones in pt_workloads.h) ----
  * Camera rays of pt_rays_camera; bounce rays from closest hits: origin at the hit, a

@@ -30,12 +30,16 @@ def oracle():
     return Oracle()
 
 
-@pytest.fixture(params=[1, 0], ids=["wide", "binary"])
+@pytest.fixture(params=[(1, 1), (1, 0), (0, 1)], ids=["wide-phased", "wide-loop", "binary"])
 def layout(request):
-    """Runs a test with the four-wide and with the two-wide node layout."""
-    pt.query_layout(request.param)
+    """Runs a test with each traversal form: four-wide nodes walked in node/leaf phases or in one
+    loop, and the two-wide re-layout of the caller's tree."""
+    wide, spec = request.param
+    pt.query_layout(wide)
+    pt.query_walk(spec)
     yield request.param
     pt.query_layout(1)
+    pt.query_walk(1)
 
 
 def assert_hits_equal(got, want):
