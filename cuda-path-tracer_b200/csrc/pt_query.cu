@@ -391,6 +391,86 @@ pt_status pt_query_walk(int speculative) {
     return guard([&]() { g_query_config.speculative = speculative ? 1 : 0; });
 }
 
+// ---- no-allocation query ---------------------------------------------------------------------
+// Scratch of pt_query_rays_static, shared by every call on a device: the persistent kernel's
+// ray counter, then staging for PT_STATIC_QUERY_MAX_RAYS rays, tmax values, hits and counters.
+namespace {
+constexpr size_t kStaticRays = PT_STATIC_QUERY_MAX_RAYS;
+constexpr size_t kStaticRaysOffset = 256;
+constexpr size_t kStaticTmaxOffset = kStaticRaysOffset + kStaticRays * sizeof(pt_ray);
+constexpr size_t kStaticHitsOffset = kStaticTmaxOffset + kStaticRays * sizeof(float);
+constexpr size_t kStaticStatsOffset = kStaticHitsOffset + kStaticRays * sizeof(pt_hit);
+constexpr size_t kStaticScratchBytes = kStaticStatsOffset + kStaticRays * sizeof(pt_ray_stats);
+static_assert(kStaticHitsOffset % 16 == 0 && kStaticStatsOffset % 8 == 0, "scratch alignment");
+}
+
+static __device__ __align__(256) unsigned char g_static_query_scratch[kStaticScratchBytes];
+
+namespace {
+// Device address of g_static_query_scratch, looked up once per device with that device current.
+std::mutex g_static_mutex;
+unsigned char *g_static_address[64] = {nullptr};
+
+unsigned char *static_scratch() {
+    int dev = 0;
+    PT_CUDA(cudaGetDevice(&dev));
+    if(dev < 0 || dev >= 64) throw Error(PT_INVALID_ARGUMENT, "device index beyond 63");
+    std::lock_guard<std::mutex> lock(g_static_mutex);
+    if(!g_static_address[dev]) {
+        void *ptr = nullptr;
+        cudaError_t st = cudaGetSymbolAddress(&ptr, g_static_query_scratch);
+        if(st != cudaSuccess) throw Error(PT_CUDA_ERROR, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(st));
+        g_static_address[dev] = static_cast<unsigned char *>(ptr);
+    }
+    return g_static_address[dev];
+}
+} // namespace
+
+// Callers that cannot let a library allocate device memory get this form of pt_query_rays: no
+// cudaMalloc or cudaFree, no streams or events created; it stages through the static array above.
+pt_status pt_query_rays_static(const pt_scene *scene, const pt_ray *rays, size_t count, int mode, float tmin,
+                               const float *tmax, pt_hit *hits, pt_ray_stats *stats, void *stream) {
+    return guard([&]() {
+        if(!scene || (count && (!rays || !hits))) throw Error(PT_INVALID_ARGUMENT, "null argument");
+        if(mode != PT_QUERY_CLOSEST && mode != PT_QUERY_ANY) throw Error(PT_INVALID_ARGUMENT, "unknown query mode");
+        if(count > kStaticRays)
+            throw Error(PT_INVALID_ARGUMENT, "pt_query_rays_static takes at most " + std::to_string(kStaticRays) +
+                                                 " rays per call (its static scratch); got " + std::to_string(count));
+        if(!count) return;
+        unsigned char *base = static_scratch();
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        unsigned long long *counter = reinterpret_cast<unsigned long long *>(base);
+        pt_ray *d_rays = reinterpret_cast<pt_ray *>(base + kStaticRaysOffset);
+        float *d_tmax = tmax ? reinterpret_cast<float *>(base + kStaticTmaxOffset) : nullptr;
+        pt_hit *d_hits = reinterpret_cast<pt_hit *>(base + kStaticHitsOffset);
+        pt_ray_stats *d_stats = stats ? reinterpret_cast<pt_ray_stats *>(base + kStaticStatsOffset) : nullptr;
+        PT_CUDA(cudaMemcpyAsync(d_rays, rays, count * sizeof(pt_ray), cudaMemcpyHostToDevice, st));
+        if(tmax) PT_CUDA(cudaMemcpyAsync(d_tmax, tmax, count * sizeof(float), cudaMemcpyHostToDevice, st));
+        PT_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st));   // the counter must start at zero
+        const DeviceScene &s = scene->view;
+        const bool wide = s.nodes4 != nullptr;
+        const bool any = mode == PT_QUERY_ANY;
+        using Fn = void (*)(DeviceScene, const pt_ray *, size_t, float, const float *, pt_hit *, pt_ray_stats *, int,
+                            unsigned long long *, int);
+        static const Fn table[8] = {
+            query_persistent_kernel<false, false, 0>, query_persistent_kernel<false, false, 2>,
+            query_persistent_kernel<false, true, 0>, query_persistent_kernel<false, true, 2>,
+            query_persistent_kernel<true, false, 0>, query_persistent_kernel<true, false, 2>,
+            query_persistent_kernel<true, true, 0>, query_persistent_kernel<true, true, 2>};
+        Fn fn = table[(any ? 4 : 0) + (stats ? 2 : 0) + (wide ? 1 : 0)];
+        const size_t smem = wide ? size_t(kSharedStack4) * kQueryBlock * sizeof(int2) : size_t(kSharedStack) * kQueryBlock * sizeof(int32_t);
+        int per_sm = 0;
+        PT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)fn, kQueryBlock, smem));
+        size_t want = (count + kQueryBlock - 1) / kQueryBlock;
+        unsigned grid = unsigned(std::min<size_t>(want, size_t(device_sm_count()) * size_t(per_sm > 0 ? per_sm : 1)));
+        fn<<<grid, kQueryBlock, smem, st>>>(s, d_rays, count, tmin, d_tmax, d_hits, d_stats, kTieLowestId, counter, 16);
+        PT_CUDA(cudaGetLastError());
+        PT_CUDA(cudaMemcpyAsync(hits, d_hits, count * sizeof(pt_hit), cudaMemcpyDeviceToHost, st));
+        if(stats) PT_CUDA(cudaMemcpyAsync(stats, d_stats, count * sizeof(pt_ray_stats), cudaMemcpyDeviceToHost, st));
+        PT_CUDA(cudaStreamSynchronize(st));
+    });
+}
+
 pt_status pt_rays_camera_device(const pt_camera *camera, int width, int height, uint64_t seed, uint64_t first,
                                 size_t count, pt_ray *rays, void *stream) {
     return guard([&]() {

@@ -134,6 +134,21 @@ pt_status pt_query_rays_device(const pt_scene *scene, const pt_ray *rays, size_t
 /* Host buffers: uploads, traces and downloads in overlapped chunks; returns when `hits` is filled. */
 pt_status pt_query_rays(const pt_scene *scene, const pt_ray *rays, size_t count, int mode,
                         float tmin, const float *tmax, pt_hit *hits, pt_ray_stats *stats);
+/* Host-buffer query that allocates nothing.  Some callers cannot let a library call cudaMalloc
+ * or cudaFree: applications that hand all device memory to their own pool allocator at start-up,
+ * latency-critical loops (cudaFree can synchronize the whole device and stall other streams),
+ * and processes running under a device-memory cap where a late allocation may fail.
+ * No counterpart in the reference.  It answers exactly like pt_query_rays but stages the rays,
+ * tmax values, hits and counters through one static device array of the library (about 3.7 MB,
+ * held by every GPU that loads the library until the process exits), so a call takes at most
+ * PT_STATIC_QUERY_MAX_RAYS rays (more is PT_INVALID_ARGUMENT) and waits for its own work on
+ * `stream` (a cudaStream_t; 0 = legacy default stream) before returning.  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress) with that device current.
+ * Every call shares the array: calls that overlap on the GPU (other streams, other host threads)
+ * race on it. */
+#define PT_STATIC_QUERY_MAX_RAYS 65536
+pt_status pt_query_rays_static(const pt_scene *scene, const pt_ray *rays, size_t count, int mode,
+                               float tmin, const float *tmax, pt_hit *hits, pt_ray_stats *stats, void *stream);
 /* Compatibility form of cuda_query_rays(scene, rays, brute) (src/cuda/cuda_renderer.cu:248-260):
  * host rays in, full 56-byte trace_result records out, t range (0.001, FLT_MAX).
  * brute != 0 scans every leaf in node-array order (src/renderer/transport.h:48-60). */

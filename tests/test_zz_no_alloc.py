@@ -1,0 +1,59 @@
+"""The query entry point that allocates nothing (pt_query_rays_static).
+
+Callers that cannot let a library allocate device memory — applications that hand all device
+memory to their own pool allocator, latency-critical loops where cudaFree's device-wide
+synchronization would stall other streams, processes under a device-memory cap — use this form
+instead of pt_query_rays.  It stages through one static device array, so it takes at most
+PT_STATIC_QUERY_MAX_RAYS rays per call.  Its answers must equal pt_query_rays's, bit for bit,
+call after call (the array keeps the previous call's contents, so a call that forgot to clear
+its counter would show up on the second call).  This file is collected last so that a run
+that stops at the first failure has already run every other test; it also passes on its own.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import ptb200 as pt
+
+pytestmark = pytest.mark.gpu
+MAX_RAYS = 65536   # PT_STATIC_QUERY_MAX_RAYS in include/pt.h
+
+
+def static_query(scene: pt.Scene, rays, mode, tmin, tmax, stats: bool):
+    lib = pt.library()
+    fn = lib.pt_query_rays_static
+    fn.restype = C.c_int
+    fn.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int, C.c_float, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    hits = np.zeros(len(rays), pt.HIT)
+    st = np.zeros(len(rays), pt.RAY_STATS) if stats else None
+    status = fn(scene.handle, rays.ctypes.data, len(rays), mode, tmin,
+                None if tmax is None else tmax.ctypes.data, hits.ctypes.data,
+                None if st is None else st.ctypes.data, None)
+    return status, hits, st
+
+
+@pytest.mark.parametrize("mode", [pt.QUERY_CLOSEST, pt.QUERY_ANY])
+def test_static_query_matches_allocating_query_twice(mode):
+    scene, cam = pt.procedural_scene(96, 60, sphere_count=4, segments=64, rings=33, seed=5)
+    dev = pt.Scene(scene)
+    for call in range(2):
+        rays = pt.camera_rays(cam, 96, 60, 11 + call, 0, MAX_RAYS if call == 0 else 20000)
+        tmax = None if mode == pt.QUERY_CLOSEST else np.full(len(rays), 12.0, np.float32)
+        status, hits, stats = static_query(dev, rays, mode, 0.001, tmax, stats=True)
+        assert status == 0, pt.library().pt_last_error()
+        want, want_stats = dev.query(rays, mode=mode, tmin=0.001, tmax=tmax, stats=True)
+        assert hits.tobytes() == want.tobytes(), f"call {call}"
+        assert stats.tobytes() == want_stats.tobytes(), f"call {call}"
+        assert (hits["primitive_type"] != 0).any()
+
+
+def test_static_query_rejects_more_than_its_scratch_holds():
+    scene, cam = pt.cornell_box(32, 20)
+    dev = pt.Scene(scene)
+    rays = pt.camera_rays(cam, 32, 20, 1, 0, MAX_RAYS + 1)
+    status, _, _ = static_query(dev, rays, pt.QUERY_CLOSEST, 0.001, None, stats=False)
+    assert status == 1
+    assert "at most 65536 rays" in pt.library().pt_last_error().decode()
