@@ -555,9 +555,9 @@ PT_HD inline bool leaf4(const DeviceScene &s, int32_t ref, const pt_ray &r, floa
 // Per-thread four-wide walk (local-memory stack), for kernels that run one ray per thread.
 template <bool kAny>
 PT_HD inline bool traverse4(const DeviceScene &s, const pt_ray &r, float tmin, float tmax, int tie,
-                            HitInfo &hit, uint32_t &boxes, uint32_t &prims, int &error) {
+                            HitInfo &hit, uint32_t &boxes, uint32_t &prims, int &error, int32_t root = 0) {
     hit.slot = -1; hit.t = 0; hit.u = 0; hit.v = 0;
-    if (s.empty || s.node_count == 0) return false;
+    if (s.empty || s.node_count == 0 || root < 0) return false;
     RayBox rb = ray_box(r);
     float dl = length(mk(r.direction));
     bool found = false;
@@ -566,7 +566,7 @@ PT_HD inline bool traverse4(const DeviceScene &s, const pt_ray &r, float tmin, f
     int32_t sref[3 * kStackCapacity];
     float sdist[3 * kStackCapacity];
     int sp = 0;
-    int32_t cur = 0;   // root node
+    int32_t cur = root;
     for (;;) {
         if (cur >= 0) {
             int32_t ref[4];
@@ -707,7 +707,9 @@ namespace ptb {
 // walking speculatively while others search — and in the leaf phase all lanes test their leaf
 // together, so node work and primitive work do not diverge inside one warp instruction
 // stream.  Same contract and answer as persistent_walk4.
-template <bool kAny, class Get, class Done>
+// With kRoot, get() also returns the walk's root node (several trees in one node array; < 0 for
+// an empty tree).
+template <bool kAny, bool kRoot = false, class Get, class Done>
 __device__ inline void persistent_walk4_spec(const DeviceScene &s, size_t count, unsigned long long *next, int min_active,
                                              int tie, Get get, Done done) {
     const size_t warp_first = (size_t(blockIdx.x) * blockDim.x + (threadIdx.x & ~31u));
@@ -751,13 +753,15 @@ __device__ inline void persistent_walk4_spec(const DeviceScene &s, size_t count,
                 size_t mine = base + __popc(idle & ((1u << lane) - 1u));
                 if (mine < count) {
                     index = mine;
-                    get(index, r, tmin, tmax);
+                    int32_t root = 0;
+                    if constexpr (kRoot) get(index, r, tmin, tmax, root);
+                    else get(index, r, tmin, tmax);
                     rb = ray_box(r);
                     dl = length(mk(r.direction));
                     closest = tmax; limit = tmax; best_key = 0;
                     hit.slot = -1; hit.t = 0; hit.u = 0; hit.v = 0;
                     boxes = 0; prims = 0; sp = 0; found = false; error = 0;
-                    cur = (s.empty || s.node_count == 0) ? kNone : 0;
+                    cur = (s.empty || s.node_count == 0 || root < 0) ? kNone : root;
                     leaf = kNone;
                     busy = true;
                 }

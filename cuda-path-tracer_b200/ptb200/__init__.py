@@ -141,6 +141,13 @@ def library() -> C.CDLL:
         "pt_rgba_image": (I, [P, P, S]),
         "pt_stats": (I, [P, P, P, P]),
         "pt_renderer_tuning": (I, [P, C.c_int32]),
+        "pt_batch_create": (I, [P, C.c_int32, P, C.c_int32, C.c_uint32, P]),
+        "pt_batch_destroy": (I, [P]),
+        "pt_batch_run": (I, [P]),
+        "pt_batch_get_sums": (I, [P, C.c_int32, P, S]),
+        "pt_batch_stats": (I, [P, P, P, P, S]),
+        "pt_batch_tuning": (I, [P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
+        "pt_batch_autotune": (I, [P, C.c_int32, C.c_char_p, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -504,3 +511,61 @@ class CudaRenderer:
 
     def rays_traced(self) -> int:
         return self._stats()[2]
+
+
+# ---------------------------------------------------------------- batched rendering
+JOB = np.dtype([("scene", "<i4"), ("width", "<i4"), ("height", "<i4"), ("samples", "<i4"), ("max_depth", "<i4"),
+                ("pad", "<i4"), ("seed", "<u8"), ("camera", CAMERA), ("tail", "<u4")])
+assert JOB.itemsize == 120, JOB.itemsize
+
+
+class Batch:
+    """Many render jobs in one launch (pt_batch_*).  ``jobs`` are dicts with keys scene (index),
+    camera, width, height, samples, max_depth, seed."""
+
+    def __init__(self, scenes, jobs, direct_light: bool = True):
+        self._scenes = list(scenes)
+        descs = (_SceneDesc * len(self._scenes))(*[s.desc() for s in self._scenes])
+        arr = np.zeros(len(jobs), JOB)
+        for k, j in enumerate(jobs):
+            arr[k]["scene"], arr[k]["width"], arr[k]["height"] = j["scene"], j["width"], j["height"]
+            arr[k]["samples"], arr[k]["max_depth"], arr[k]["seed"] = j["samples"], j["max_depth"], j["seed"]
+            arr[k]["camera"] = np.asarray(j["camera"], CAMERA).reshape(-1)[0]
+        self.jobs = arr
+        self._h = C.c_void_p()
+        check(library().pt_batch_create(descs, len(self._scenes), arr.ctypes.data, len(arr),
+                                        RENDER_MIS if direct_light else 0, C.byref(self._h)))
+
+    def close(self):
+        if self._h:
+            library().pt_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self) -> None:
+        check(library().pt_batch_run(self._h))
+
+    def tuning(self, path_capacity=0, block=256, min_active=16, tail_paths=16384, use_graph=1) -> None:
+        check(library().pt_batch_tuning(self._h, path_capacity, block, min_active, tail_paths, use_graph))
+
+    def autotune(self, probe_samples: int = 1, cache_path: str | None = None):
+        best = (C.c_int32 * 4)()
+        check(library().pt_batch_autotune(self._h, probe_samples, cache_path.encode() if cache_path else None, best))
+        return tuple(best)
+
+    def sums(self, job: int) -> np.ndarray:
+        j = self.jobs[job]
+        out = np.zeros(int(j["width"]) * int(j["height"]) * 3, np.float32)
+        check(library().pt_batch_get_sums(self._h, job, out.ctypes.data, out.size))
+        return out
+
+    def stats(self):
+        ms, rays = C.c_float(), C.c_uint64()
+        done = np.zeros(len(self.jobs), np.float64)
+        check(library().pt_batch_stats(self._h, C.byref(ms), C.byref(rays), done.ctypes.data, len(done)))
+        return ms.value, rays.value, done

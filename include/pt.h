@@ -215,6 +215,38 @@ pt_status pt_rgba_image(const pt_renderer *renderer, unsigned char *host_pixels,
 /* sample_count(), kernel_milliseconds(), rays_traced(). */
 pt_status pt_stats(const pt_renderer *renderer, int *samples, float *kernel_ms, uint64_t *rays);
 
+/* ---- batched rendering ----
+ * Many render jobs — each its own scene, camera, resolution, sample count, bounce limit and seed —
+ * rendered together: every job's scene is merged into one device scene and a pool of path slots
+ * walks all jobs' pixels inside one CUDA graph launch (a device-side loop of wavefront
+ * iterations, then a fused kernel for the tail).  Each job's sums equal those of a pt_renderer
+ * rendering that job alone (MIS flag as given, debug views not supported).  No counterpart in the
+ * reference, which renders one image per cuda_renderer. */
+typedef struct pt_job {
+    int32_t scene;              /* index into the scene list of pt_batch_create */
+    int32_t width, height, samples, max_depth;
+    uint64_t seed;
+    pt_camera camera;
+} pt_job;
+typedef struct pt_batch pt_batch;
+pt_status pt_batch_create(const pt_scene_desc *scenes, int32_t scene_count, const pt_job *jobs, int32_t job_count,
+                          uint32_t flags, pt_batch **out);
+pt_status pt_batch_destroy(pt_batch *batch);
+/* Renders every job's samples from a fresh state (sums zeroed, streams seeded); blocks. */
+pt_status pt_batch_run(pt_batch *batch);
+pt_status pt_batch_get_sums(const pt_batch *batch, int32_t job, float *rgb_sums, size_t floats);
+/* Device time of the last run, rays traced, and each job's completion time from the run's start. */
+pt_status pt_batch_stats(const pt_batch *batch, float *kernel_ms, uint64_t *rays, double *job_completion_ms, size_t jobs);
+/* path_capacity: path slots (0 = min(pixels, 2^22)); block: 64, 128 or 256 threads; min_active:
+ * traversal refill threshold; tail_paths: live paths below which the fused kernel finishes;
+ * use_graph: 1 = one graph launch with a device-side loop, 0 = host-driven loop. */
+pt_status pt_batch_tuning(pt_batch *batch, int32_t path_capacity, int32_t block, int32_t min_active, int32_t tail_paths,
+                          int32_t use_graph);
+/* Sweeps capacity x block x min_active x graph on probe runs (each job at min(probe_samples, its
+ * samples)), applies the fastest and caches it per (log2 triangles, log2 pixels) bucket in
+ * `cache_path` (NULL: no cache).  best = {capacity, block, min_active, use_graph}. */
+pt_status pt_batch_autotune(pt_batch *batch, int32_t probe_samples, const char *cache_path, int32_t *best);
+
 #ifdef __cplusplus
 }
 #endif
