@@ -46,6 +46,9 @@ def parse():
     ap.add_argument("--log2-rays", type=int, default=LOG2_RAYS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--workload", choices=["query", "batch48"], default="query",
+                    help="query: the closest-hit benchmark (default); batch48: 48 render jobs in one launch")
+    ap.add_argument("--jobs", type=int, default=48)
     return ap.parse_args()
 
 
@@ -164,10 +167,61 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def batch_jobs(count: int):
+    """Seeded render jobs 1..count: log-uniform 10k-2M triangles and 256x256-1920x1080 pixels,
+    8-64 spp, bounce limit 4-12, scenes in the style of the procedural 1M-triangle scene."""
+    scenes, jobs = [], []
+    for i in range(1, count + 1):
+        g = np.random.default_rng(1000 + i)
+        tris = float(np.exp(g.uniform(np.log(1e4), np.log(2e6))))
+        area = float(np.exp(g.uniform(np.log(256 * 256), np.log(1920 * 1080))))
+        aspect = float(g.choice([1.0, 4.0 / 3.0, 16.0 / 9.0]))
+        w = int(min(1920, max(256, round(np.sqrt(area * aspect)))))
+        h = int(min(1080, max(256, round(area / w))))
+        spheres = int(min(30, max(1, round(tris / 65536))))
+        seg = int(max(8, round(np.sqrt(tris / spheres))))
+        scene, cam = pt.procedural_scene(w, h, sphere_count=spheres, segments=seg, rings=max(3, seg // 2 + 1), seed=i)
+        scenes.append(scene)
+        jobs.append(dict(scene=i - 1, camera=cam, width=w, height=h, samples=int(g.integers(8, 65)),
+                         max_depth=int(g.integers(4, 13)), seed=i))
+    return scenes, jobs
+
+
+def run_batch(args):
+    """48 jobs in one graph-captured launch (after a probe autotune); prints one JSON line."""
+    import torch
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    t = time.perf_counter()
+    scenes, jobs = batch_jobs(args.jobs)
+    build_s = time.perf_counter() - t
+    b = pt.Batch(scenes, jobs)
+    best = b.autotune(probe_samples=1, cache_path=None)
+    for _ in range(max(1, args.warmup // 3)):
+        b.run()
+    clocks = Clocks(int(os.environ.get("LOCAL_RANK", "0")))
+    b.run()
+    clock = clocks.stop()
+    ms, rays, done = b.stats()
+    line = {"metric": "Mrays/s batched render", "value": rays / ms / 1e3, "unit": "Mrays/s", "n_gpus": 1, "steps": 1,
+            "warmup": max(1, args.warmup // 3), "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"{len(jobs)} render jobs in one graph launch", "jobs": len(jobs),
+                       "triangles": int(sum(len(s.triangles) for s in scenes)),
+                       "pixels": int(sum(j["width"] * j["height"] for j in jobs)),
+                       "samples": int(sum(j["width"] * j["height"] * j["samples"] for j in jobs)),
+                       "autotuned": {"path_capacity": best[0], "block": best[1], "min_active": best[2], "graph": best[3]}},
+            "rays": rays, "job_completion_ms": [round(float(x), 3) for x in done], "scene_build_s": build_s,
+            "clocks": clock}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.workload == "batch48":
+        run_batch(args)
         return
     import torch
     import torch.distributed as dist
