@@ -1,0 +1,631 @@
+// pt_mlp.cu — the radiance-cache MLP on the 5th-generation tensor cores (tcgen05, sm_100a).
+//
+// Network: 64 inputs (position frequency encoding 3x12, spherical harmonics of the direction up
+// to degree 3 = 16 coefficients, normal, albedo, roughness = 7; zero padded), five hidden layers
+// of 64 with ReLU, 3 outputs with exp.  BF16 weights and activations, FP32 accumulation in TMEM.
+// No counterpart in the reference (it has no learned component).
+//
+// Shared-memory operand layout (one convention for every matrix): a R x C bf16 matrix is stored
+// as 8-row x 8-column core matrices of 128 contiguous bytes; element (r, c) sits at byte
+//   (r % 8) * 16 + (r / 8) * (C / 8) * 128 + (c % 8) * 2 + (c / 8) * 128.
+// Read with rows as M/N and columns as K it is the canonical K-major no-swizzle layout
+// (LBO = 128 B between K core matrices, SBO = C*16 B between row groups); read transposed it is
+// the canonical MN-major layout (SBO = 128 B, LBO = C*16 B).  So activations, gradients and
+// weights are each stored once and used both ways: X*W, dZ*W^T and X^T*dZ.
+// Every mbarrier wait is bounded: on expiry the kernel records PT_TIMEOUT in its status word,
+// stops issuing, frees its TMEM and returns.
+#include <cmath>
+#include <cstring>
+#include <vector>
+#include <cuda_bf16.h>
+#include "pt_api_common.h"
+#include "pt_device.h"
+
+using namespace ptb;
+
+namespace ptb {
+namespace mlp {
+
+constexpr int kTile = 128;             // rows per MMA tile (queries)
+constexpr int kWidth = 64;             // input and hidden width
+constexpr int kHidden = 5;             // hidden layers (matrices 0..4 are 64x64)
+constexpr int kOut = 3;
+constexpr int kOutPad = 16;            // output layer N, padded for M = 128
+constexpr int kMatBytes = kWidth * kWidth * 2;             // 8 KB
+constexpr int kOutMatBytes = kOutPad * kWidth * 2;         // 2 KB
+constexpr int kWeightBytes = kHidden * kMatBytes + kOutMatBytes;   // 43008
+constexpr int kActBytes = kTile * kWidth * 2;              // 16 KB per 128 x 64 tile
+constexpr int kOutActBytes = kTile * kOutPad * 2;          // 4 KB per 128 x 16 tile
+constexpr int kPad = 2048;                                 // guard after every operand buffer
+constexpr int kMasterFloats = kHidden * kWidth * kWidth + kWidth * kOut;   // 20672
+constexpr long long kSpinLimit = 1ll << 22;
+
+// byte offset of element (r, c) of a matrix with `cols` columns in the core-matrix layout
+__host__ __device__ inline uint32_t canon(uint32_t r, uint32_t c, uint32_t cols) {
+    return (r % 8) * 16 + (r / 8) * (cols / 8) * 128 + (c % 8) * 2 + (c / 8) * 128;
+}
+
+__device__ inline uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// UMMA shared-memory descriptor, no swizzle, Blackwell version bit
+__device__ inline uint64_t desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+    d |= (uint64_t)1 << 46;
+    return d;
+}
+// instruction descriptor: kind::f16, BF16 x BF16 -> F32
+__host__ __device__ constexpr uint32_t idesc(int M, int N, bool a_mn, bool b_mn) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((a_mn ? 1u : 0u) << 15) | ((b_mn ? 1u : 0u) << 16) |
+           ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ inline void mma(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t id, uint32_t accumulate) {
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                 "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+                 :: "r"(d_tmem), "l"(a), "l"(b), "r"(id), "r"(accumulate));
+}
+__device__ inline void commit(uint64_t *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" :: "r"(smem_u32(bar)) : "memory");
+}
+__device__ inline void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ inline void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ inline void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ inline void wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+__device__ inline void bar_init(uint64_t *bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+// bounded wait for the phase with parity `phase` to complete
+__device__ inline bool bar_wait(uint64_t *bar, uint32_t phase) {
+    uint32_t addr = smem_u32(bar);
+    for (long long i = 0; i < kSpinLimit; i++) {
+        uint32_t done;
+        asm volatile("{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+                     "selp.b32 %0, 1, 0, P1;\n\t}\n" : "=r"(done) : "r"(addr), "r"(phase) : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// 16 consecutive FP32 columns of this thread's TMEM lane (warp w reads lanes 32w..32w+31)
+__device__ inline void tmem_ld16(uint32_t taddr, float v[16]) {
+    uint32_t r[16];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                   "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+                 : "r"(taddr));
+    wait_ld();
+#pragma unroll
+    for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+
+// writes 8 bf16 values (columns 8c..8c+7 of row r) into a core-matrix layout buffer
+__device__ inline void store8(unsigned char *base, uint32_t r, uint32_t c8, uint32_t cols, const float *x) {
+    __nv_bfloat162 p0 = __floats2bfloat162_rn(x[0], x[1]), p1 = __floats2bfloat162_rn(x[2], x[3]);
+    __nv_bfloat162 p2 = __floats2bfloat162_rn(x[4], x[5]), p3 = __floats2bfloat162_rn(x[6], x[7]);
+    uint4 v;
+    v.x = *reinterpret_cast<uint32_t *>(&p0); v.y = *reinterpret_cast<uint32_t *>(&p1);
+    v.z = *reinterpret_cast<uint32_t *>(&p2); v.w = *reinterpret_cast<uint32_t *>(&p3);
+    *reinterpret_cast<uint4 *>(base + canon(r, c8 * 8, cols)) = v;
+}
+__device__ inline void load8(const unsigned char *base, uint32_t r, uint32_t c8, uint32_t cols, float *x) {
+    uint4 v = *reinterpret_cast<const uint4 *>(base + canon(r, c8 * 8, cols));
+    const __nv_bfloat162 *p = reinterpret_cast<const __nv_bfloat162 *>(&v);
+#pragma unroll
+    for (int i = 0; i < 4; i++) { float2 f = __bfloat1622float2(p[i]); x[2 * i] = f.x; x[2 * i + 1] = f.y; }
+}
+
+// Input encoding of one query (see the file comment); 64 values, zero padded.
+__device__ inline void encode(const pt_cache_query &q, const float lo[3], const float inv_extent[3], float x[64]) {
+    const float pos[3] = {q.position.x, q.position.y, q.position.z};
+    int k = 0;
+    for (int a = 0; a < 3; a++) {
+        float p = (pos[a] - lo[a]) * inv_extent[a];
+        float s = 3.14159265358979f * p;
+        for (int f = 0; f < 6; f++) {
+            float sn, cs;
+            sincosf(s, &sn, &cs);
+            x[k++] = sn; x[k++] = cs;
+            s *= 2.0f;
+        }
+    }
+    float dx = q.direction.x, dy = q.direction.y, dz = q.direction.z;
+    float xx = dx * dx, yy = dy * dy, zz = dz * dz;
+    x[k++] = 0.28209479177387814f;
+    x[k++] = -0.48860251190291987f * dy;
+    x[k++] = 0.48860251190291987f * dz;
+    x[k++] = -0.48860251190291987f * dx;
+    x[k++] = 1.0925484305920792f * dx * dy;
+    x[k++] = -1.0925484305920792f * dy * dz;
+    x[k++] = 0.31539156525252005f * (3.0f * zz - 1.0f);
+    x[k++] = -1.0925484305920792f * dx * dz;
+    x[k++] = 0.5462742152960396f * (xx - yy);
+    x[k++] = -0.5900435899266435f * dy * (3.0f * xx - yy);
+    x[k++] = 2.890611442640554f * dx * dy * dz;
+    x[k++] = -0.4570457994644658f * dy * (5.0f * zz - 1.0f);
+    x[k++] = 0.3731763325901154f * dz * (5.0f * zz - 3.0f);
+    x[k++] = -0.4570457994644658f * dx * (5.0f * zz - 1.0f);
+    x[k++] = 1.445305721320277f * dz * (xx - yy);
+    x[k++] = -0.5900435899266435f * dx * (xx - 3.0f * yy);
+    x[k++] = q.normal.x; x[k++] = q.normal.y; x[k++] = q.normal.z;
+    x[k++] = q.albedo.x; x[k++] = q.albedo.y; x[k++] = q.albedo.z;
+    x[k++] = q.roughness;
+    while (k < 64) x[k++] = 0.0f;
+}
+
+struct Scratch {                // per-CTA shared memory header
+    uint64_t bar;
+    uint32_t tmem;
+    uint32_t pad[13];
+};
+
+__device__ inline void tmem_alloc(Scratch *h, uint32_t cols) {
+    if (threadIdx.x < 32) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" :: "r"(smem_u32(&h->tmem)), "r"(cols) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+}
+__device__ inline void tmem_free(uint32_t base, uint32_t cols) {
+    if (threadIdx.x < 32) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(base), "r"(cols) : "memory");
+}
+
+// Copies the canonical BF16 weights (global) into shared memory.
+__device__ inline void load_weights(unsigned char *w, const unsigned char *g) {
+    for (int i = threadIdx.x; i < kWeightBytes / 16; i += blockDim.x)
+        reinterpret_cast<uint4 *>(w)[i] = reinterpret_cast<const uint4 *>(g)[i];
+}
+
+// X (128 x 64, rows = queries) into the core-matrix layout; rows past `count` are zero.
+__device__ inline void encode_tile(unsigned char *x, const pt_cache_query *q, size_t first, size_t count, const float lo[3],
+                                   const float inv_extent[3]) {
+    float v[64];
+    size_t row = first + threadIdx.x;
+    if (row < count) encode(q[row], lo, inv_extent, v);
+    else for (int i = 0; i < 64; i++) v[i] = 0.0f;
+    for (int c = 0; c < 8; c++) store8(x, threadIdx.x, c, 64, v + 8 * c);
+}
+
+// D[128 x N] (+)= A[128 x K] * B[N x K]^T, A and B K-major in the core layout, K = 16 per MMA.
+__device__ inline void mma_kk(uint32_t d, const unsigned char *a, uint32_t a_cols, const unsigned char *b, uint32_t b_cols,
+                              int N, int K, bool accumulate) {
+    for (int s = 0; s < K / 16; s++) {
+        uint64_t da = desc(smem_u32(a) + s * 256, 128, a_cols * 16);
+        uint64_t db = desc(smem_u32(b) + s * 256, 128, b_cols * 16);
+        mma(d, da, db, idesc(kTile, N, false, false), (accumulate || s) ? 1u : 0u);
+    }
+}
+// D[128 x N] (+)= A[128 x K] * B where B is stored as [K rows x N cols] (core layout): B read
+// MN-major.  A K-major with a_cols = K.
+__device__ inline void mma_kmn(uint32_t d, const unsigned char *a, uint32_t a_cols, const unsigned char *b, uint32_t b_cols,
+                               int N, int K, bool accumulate) {
+    for (int s = 0; s < K / 16; s++) {
+        uint64_t da = desc(smem_u32(a) + s * 256, 128, a_cols * 16);
+        uint64_t db = desc(smem_u32(b) + s * 2 * b_cols * 16, b_cols * 16, 128);
+        mma(d, da, db, idesc(kTile, N, false, true), (accumulate || s) ? 1u : 0u);
+    }
+}
+// D[128(64 valid) x N] (+)= A^T * B with A [128 rows m x 64 cols k] and B [128 rows m x N cols],
+// both read MN-major (the reduction runs over the 128 rows m).
+__device__ inline void mma_tn(uint32_t d, const unsigned char *a, const unsigned char *b, uint32_t b_cols, int N, bool accumulate) {
+    for (int s = 0; s < kTile / 16; s++) {
+        uint64_t da = desc(smem_u32(a) + s * 2 * 64 * 16, 64 * 16, 128);
+        uint64_t db = desc(smem_u32(b) + s * 2 * b_cols * 16, b_cols * 16, 128);
+        mma(d, da, db, idesc(kTile, N, true, true), (accumulate || s) ? 1u : 0u);
+    }
+}
+
+// Issues with thread 0, commits to the barrier and waits (all threads).  Returns false on timeout.
+struct Sync {
+    Scratch *h;
+    uint32_t phase = 0;
+    __device__ bool wait_all() {
+        if (threadIdx.x == 0) commit(&h->bar);
+        bool ok = bar_wait(&h->bar, phase);
+        phase ^= 1;
+        fence_after();
+        return ok;
+    }
+};
+
+// ---- forward (query) -----------------------------------------------------------------------
+// smem: header | W (43008) | pad | X | pad | H | pad
+constexpr size_t kFwdSmem = 256 + kWeightBytes + kPad + 2 * (kActBytes + kPad);
+
+__global__ void __launch_bounds__(kTile, 1) forward_kernel(const unsigned char *weights, const pt_cache_query *queries, size_t count,
+                                                           float3 lo, float3 hi, float *out, int *status) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    Scratch *h = reinterpret_cast<Scratch *>(smem);
+    unsigned char *w = smem + 256;
+    unsigned char *bufx = w + kWeightBytes + kPad;
+    unsigned char *bufh = bufx + kActBytes + kPad;
+    const float l[3] = {lo.x, lo.y, lo.z};
+    const float ie[3] = {1.0f / fmaxf(hi.x - lo.x, 1e-30f), 1.0f / fmaxf(hi.y - lo.y, 1e-30f), 1.0f / fmaxf(hi.z - lo.z, 1e-30f)};
+    if (threadIdx.x == 0) bar_init(&h->bar);
+    tmem_alloc(h, 128);
+    load_weights(w, weights);
+    fence_async_smem();
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tbase = h->tmem;
+    const uint32_t lane_base = tbase + ((uint32_t)(threadIdx.x & ~31u) << 16);
+    Sync sync{h};
+    bool ok = true;
+    const size_t tiles = (count + kTile - 1) / kTile;
+    for (size_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
+        encode_tile(bufx, queries, t * kTile, count, l, ie);
+        fence_async_smem();
+        fence_before();
+        __syncthreads();
+        fence_after();
+        unsigned char *in = bufx, *outb = bufh;
+        for (int layer = 0; layer < kHidden && ok; layer++) {
+            if (threadIdx.x == 0) mma_kk(tbase, in, 64, w + layer * kMatBytes, 64, 64, 64, false);
+            ok = sync.wait_all();
+            if (!ok) break;
+            for (int c = 0; c < 4; c++) {
+                float v[16];
+                tmem_ld16(lane_base + c * 16, v);
+                for (int i = 0; i < 16; i++) v[i] = fmaxf(v[i], 0.0f);
+                store8(outb, threadIdx.x, 2 * c, 64, v);
+                store8(outb, threadIdx.x, 2 * c + 1, 64, v + 8);
+            }
+            fence_async_smem();
+            fence_before();
+            __syncthreads();
+            fence_after();
+            unsigned char *tmp = in; in = outb; outb = tmp;
+        }
+        if (!ok) break;
+        if (threadIdx.x == 0) mma_kk(tbase + 64, in, 64, w + kHidden * kMatBytes, 64, kOutPad, 64, false);
+        ok = sync.wait_all();
+        if (!ok) break;
+        float v[16];
+        tmem_ld16(lane_base + 64, v);
+        size_t row = t * kTile + threadIdx.x;
+        if (row < count) { out[3 * row] = expf(v[0]); out[3 * row + 1] = expf(v[1]); out[3 * row + 2] = expf(v[2]); }
+        fence_before();
+        __syncthreads();
+        fence_after();
+    }
+    if (!ok && threadIdx.x == 0) atomicExch(status, int(PT_TIMEOUT));
+    fence_before();
+    __syncthreads();
+    tmem_free(tbase, 128);
+}
+
+// ---- training (forward + relative-L2 loss + backward) --------------------------------------
+// TMEM columns: [0,64) forward scratch, [64,80) output, [96,112) dW5, [128,192) dH scratch,
+// [192 + 64 l, 256 + 64 l) dW_l for l = 0..4.
+// smem: header | W | pad | H0..H5 (each + pad) | dZ + pad | dZ5 + pad
+constexpr size_t kTrainSmem = 256 + kWeightBytes + kPad + 6 * (kActBytes + kPad) + (kActBytes + kPad) + (kOutActBytes + kPad);
+
+__global__ void __launch_bounds__(kTile, 1) train_kernel(const unsigned char *weights, const pt_cache_query *queries,
+                                                         const float *targets, size_t count, float3 lo, float3 hi,
+                                                         float grad_scale, float *partial, float *loss_partial, int *status) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    Scratch *h = reinterpret_cast<Scratch *>(smem);
+    unsigned char *w = smem + 256;
+    unsigned char *act[6];
+    act[0] = w + kWeightBytes + kPad;
+    for (int i = 1; i < 6; i++) act[i] = act[i - 1] + kActBytes + kPad;
+    unsigned char *dz = act[5] + kActBytes + kPad;
+    unsigned char *dz5 = dz + kActBytes + kPad;
+    const float l[3] = {lo.x, lo.y, lo.z};
+    const float ie[3] = {1.0f / fmaxf(hi.x - lo.x, 1e-30f), 1.0f / fmaxf(hi.y - lo.y, 1e-30f), 1.0f / fmaxf(hi.z - lo.z, 1e-30f)};
+    if (threadIdx.x == 0) bar_init(&h->bar);
+    tmem_alloc(h, 512);
+    load_weights(w, weights);
+    fence_async_smem();
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tbase = h->tmem;
+    const uint32_t lane_base = tbase + ((uint32_t)(threadIdx.x & ~31u) << 16);
+    Sync sync{h};
+    bool ok = true, first = true;
+    float loss = 0.0f;
+    const size_t tiles = (count + kTile - 1) / kTile;
+    for (size_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
+        const size_t row = t * kTile + threadIdx.x;
+        encode_tile(act[0], queries, t * kTile, count, l, ie);
+        fence_async_smem();
+        fence_before();
+        __syncthreads();
+        fence_after();
+        for (int layer = 0; layer < kHidden && ok; layer++) {
+            if (threadIdx.x == 0) mma_kk(tbase, act[layer], 64, w + layer * kMatBytes, 64, 64, 64, false);
+            ok = sync.wait_all();
+            if (!ok) break;
+            for (int c = 0; c < 4; c++) {
+                float v[16];
+                tmem_ld16(lane_base + c * 16, v);
+                for (int i = 0; i < 16; i++) v[i] = fmaxf(v[i], 0.0f);
+                store8(act[layer + 1], threadIdx.x, 2 * c, 64, v);
+                store8(act[layer + 1], threadIdx.x, 2 * c + 1, 64, v + 8);
+            }
+            fence_async_smem();
+            fence_before();
+            __syncthreads();
+            fence_after();
+        }
+        if (!ok) break;
+        if (threadIdx.x == 0) mma_kk(tbase + 64, act[5], 64, w + kHidden * kMatBytes, 64, kOutPad, 64, false);
+        ok = sync.wait_all();
+        if (!ok) break;
+        {
+            // relative L2 loss, sum_c (y - t)^2 / (sg(y)^2 + 0.01) with y = exp(z): dL/dz = 2 (y - t) y / (y^2 + 0.01)
+            float v[16], g[16];
+            tmem_ld16(lane_base + 64, v);
+            for (int i = 0; i < 16; i++) g[i] = 0.0f;
+            if (row < count) {
+                for (int c = 0; c < kOut; c++) {
+                    float y = expf(v[c]), target = targets[3 * row + c];
+                    float denom = y * y + 0.01f, diff = y - target;
+                    loss += diff * diff / denom;
+                    g[c] = grad_scale * 2.0f * diff * y / denom;
+                }
+            }
+            store8(dz5, threadIdx.x, 0, kOutPad, g);
+            store8(dz5, threadIdx.x, 1, kOutPad, g + 8);
+        }
+        fence_async_smem();
+        fence_before();
+        __syncthreads();
+        fence_after();
+        // dW5 += H5^T dZ5 ; dH5 = dZ5 W5^T
+        if (threadIdx.x == 0) {
+            mma_tn(tbase + 96, act[5], dz5, kOutPad, kOutPad, !first);
+            mma_kmn(tbase + 128, dz5, kOutPad, w + kHidden * kMatBytes, 64, 64, kOutPad, false);
+        }
+        ok = sync.wait_all();
+        if (!ok) break;
+        for (int layer = kHidden - 1; layer >= 0 && ok; layer--) {
+            // dZ_layer = dH_{layer+1} * [H_{layer+1} > 0]
+            for (int c = 0; c < 4; c++) {
+                float v[16], a[16];
+                tmem_ld16(lane_base + 128 + c * 16, v);
+                load8(act[layer + 1], threadIdx.x, 2 * c, 64, a);
+                load8(act[layer + 1], threadIdx.x, 2 * c + 1, 64, a + 8);
+                for (int i = 0; i < 16; i++) v[i] = a[i] > 0.0f ? v[i] : 0.0f;
+                store8(dz, threadIdx.x, 2 * c, 64, v);
+                store8(dz, threadIdx.x, 2 * c + 1, 64, v + 8);
+            }
+            fence_async_smem();
+            fence_before();
+            __syncthreads();
+            fence_after();
+            if (threadIdx.x == 0) {
+                mma_tn(tbase + 192 + 64 * layer, act[layer], dz, 64, 64, !first);        // dW_layer += H^T dZ
+                if (layer > 0) mma_kmn(tbase + 128, dz, 64, w + layer * kMatBytes, 64, 64, 64, false);   // dH = dZ W^T
+            }
+            ok = sync.wait_all();
+        }
+        first = false;
+    }
+    // per-CTA partial gradients (rows k of the dW accumulators live in TMEM lanes 0..63)
+    float *mine = partial + size_t(blockIdx.x) * kMasterFloats;
+    if (ok) {
+        for (int layer = 0; layer < kHidden; layer++) {
+            for (int c = 0; c < 4; c++) {
+                float v[16];
+                tmem_ld16(lane_base + 192 + 64 * layer + c * 16, v);
+                if (threadIdx.x < 64)
+                    for (int i = 0; i < 16; i++) mine[layer * 4096 + threadIdx.x * 64 + c * 16 + i] = first ? 0.0f : v[i];
+            }
+        }
+        float v[16];
+        tmem_ld16(lane_base + 96, v);
+        if (threadIdx.x < 64)
+            for (int i = 0; i < kOut; i++) mine[kHidden * 4096 + threadIdx.x * kOut + i] = first ? 0.0f : v[i];
+    }
+    // loss partial
+    for (int o = 16; o; o >>= 1) loss += __shfl_down_sync(0xffffffffu, loss, o);
+    __shared__ float warp_loss[4];
+    if ((threadIdx.x & 31) == 0) warp_loss[threadIdx.x >> 5] = loss;
+    __syncthreads();
+    if (threadIdx.x == 0) loss_partial[blockIdx.x] = warp_loss[0] + warp_loss[1] + warp_loss[2] + warp_loss[3];
+    if (!ok && threadIdx.x == 0) atomicExch(status, int(PT_TIMEOUT));
+    fence_before();
+    __syncthreads();
+    tmem_free(tbase, 512);
+}
+
+// Sums the per-CTA partials in a fixed order (deterministic) into `grad`.
+__global__ void reduce_kernel(const float *partial, int ctas, float *grad) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= kMasterFloats) return;
+    float s = 0.0f;
+    for (int c = 0; c < ctas; c++) s += partial[size_t(c) * kMasterFloats + i];
+    grad[i] = s;
+}
+
+// FP32 master weight i -> its bf16 position in the canonical buffer.
+__host__ __device__ inline uint32_t master_to_canon(int i) {
+    if (i < kHidden * 4096) {
+        int layer = i / 4096, k = (i % 4096) / 64, n = i % 64;          // master W[k][n], stored as Wt rows n cols k
+        return uint32_t(layer * kMatBytes) + canon(uint32_t(n), uint32_t(k), 64);
+    }
+    int j = i - kHidden * 4096, k = j / kOut, n = j % kOut;
+    return uint32_t(kHidden * kMatBytes) + canon(uint32_t(n), uint32_t(k), 64);
+}
+
+// Adam (bias-corrected) on the FP32 masters; writes the bf16 canonical copy.
+__global__ void adam_kernel(float *master, float *m, float *v, const float *grad, int step, float lr, float beta1, float beta2,
+                            float eps, unsigned char *canon_out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= kMasterFloats) return;
+    float g = grad[i];
+    float mi = beta1 * m[i] + (1.0f - beta1) * g;
+    float vi = beta2 * v[i] + (1.0f - beta2) * g * g;
+    m[i] = mi; v[i] = vi;
+    float mh = mi / (1.0f - powf(beta1, float(step))), vh = vi / (1.0f - powf(beta2, float(step)));
+    float w = master[i] - lr * mh / (sqrtf(vh) + eps);
+    master[i] = w;
+    *reinterpret_cast<__nv_bfloat16 *>(canon_out + master_to_canon(i)) = __float2bfloat16_rn(w);
+}
+
+__global__ void canon_kernel(const float *master, unsigned char *canon_out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= kMasterFloats) return;
+    *reinterpret_cast<__nv_bfloat16 *>(canon_out + master_to_canon(i)) = __float2bfloat16_rn(master[i]);
+}
+
+} // namespace mlp
+} // namespace ptb
+
+using namespace ptb::mlp;
+
+struct pt_cache {
+    DeviceBuffer master, adam_m, adam_v, grad, weights, partial, loss_partial, status;
+    float lo[3], hi[3];
+    int step = 0;
+    int ctas = 0;
+    float lr = 1e-2f, beta1 = 0.9f, beta2 = 0.99f, eps = 1e-8f;
+};
+
+namespace {
+void refresh_canon(pt_cache *c, cudaStream_t st) {
+    canon_kernel<<<(kMasterFloats + 255) / 256, 256, 0, st>>>(c->master.get<float>(), c->weights.get<unsigned char>());
+    PT_CUDA(cudaGetLastError());
+}
+void check_status(pt_cache *c) {
+    int status = 0;
+    PT_CUDA(cudaMemcpy(&status, c->status.get(), sizeof status, cudaMemcpyDeviceToHost));
+    if (status) {
+        PT_CUDA(cudaMemset(c->status.get(), 0, sizeof(int)));
+        throw Error(pt_status(status), "radiance-cache kernel timed out waiting for the tensor cores");
+    }
+}
+int train_grid(pt_cache *c, size_t count) {
+    size_t tiles = (count + kTile - 1) / kTile;
+    return int(std::min<size_t>(tiles ? tiles : 1, size_t(c->ctas)));
+}
+// forward/backward/reduce into c->grad; returns the summed loss
+float gradients(pt_cache *c, const pt_cache_query *q, const float *targets, size_t count, cudaStream_t st) {
+    int grid = train_grid(c, count);
+    float3 lo = make_float3(c->lo[0], c->lo[1], c->lo[2]), hi = make_float3(c->hi[0], c->hi[1], c->hi[2]);
+    float scale = 1.0f / float(count * kOut);
+    train_kernel<<<grid, kTile, kTrainSmem, st>>>(c->weights.get<unsigned char>(), q, targets, count, lo, hi, scale,
+                                                   c->partial.get<float>(), c->loss_partial.get<float>(), c->status.get<int>());
+    PT_CUDA(cudaGetLastError());
+    reduce_kernel<<<(kMasterFloats + 255) / 256, 256, 0, st>>>(c->partial.get<float>(), grid, c->grad.get<float>());
+    PT_CUDA(cudaGetLastError());
+    std::vector<float> losses(static_cast<size_t>(grid));
+    PT_CUDA(cudaMemcpyAsync(losses.data(), c->loss_partial.get(), losses.size() * sizeof(float), cudaMemcpyDeviceToHost, st));
+    PT_CUDA(cudaStreamSynchronize(st));
+    check_status(c);
+    double sum = 0;
+    for (float v : losses) sum += v;
+    return float(sum);
+}
+} // namespace
+
+extern "C" {
+
+pt_status pt_cache_create(const float scene_lo[3], const float scene_hi[3], uint64_t seed, pt_cache **out) {
+    return guard([&]() {
+        if (!scene_lo || !scene_hi || !out) throw Error(PT_INVALID_ARGUMENT, "null argument");
+        *out = nullptr;
+        require_device();
+        auto c = new pt_cache;
+        try {
+            for (int a = 0; a < 3; a++) { c->lo[a] = scene_lo[a]; c->hi[a] = scene_hi[a]; }
+            // Uniform(-sqrt(6/(fan_in+fan_out)), +) initialisation from a splitmix64 stream
+            std::vector<float> w(kMasterFloats);
+            uint64_t s = seed * 0x9E3779B97F4A7C15ull + 1;
+            auto uniform = [&]() {
+                uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+                z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+                z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+                z ^= z >> 31;
+                return double(z >> 11) * 0x1p-53;
+            };
+            for (int i = 0; i < kMasterFloats; i++) {
+                double bound = i < kHidden * 4096 ? std::sqrt(6.0 / 128.0) : std::sqrt(6.0 / 67.0);
+                w[size_t(i)] = float((2 * uniform() - 1) * bound);
+            }
+            c->master.upload(w);
+            std::vector<float> zeros(kMasterFloats, 0.0f);
+            c->adam_m.upload(zeros); c->adam_v.upload(zeros); c->grad.upload(zeros);
+            c->weights.resize(kWeightBytes);
+            PT_CUDA(cudaMemset(c->weights.get(), 0, kWeightBytes));
+            c->ctas = device_sm_count();
+            c->partial.resize(size_t(c->ctas) * kMasterFloats * sizeof(float));
+            c->loss_partial.resize(size_t(c->ctas) * sizeof(float));
+            c->status.resize(sizeof(int));
+            PT_CUDA(cudaMemset(c->status.get(), 0, sizeof(int)));
+            PT_CUDA(cudaFuncSetAttribute(forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kFwdSmem)));
+            PT_CUDA(cudaFuncSetAttribute(train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kTrainSmem)));
+            refresh_canon(c, nullptr);
+            PT_CUDA(cudaDeviceSynchronize());
+        } catch (...) { delete c; throw; }
+        *out = c;
+    });
+}
+
+pt_status pt_cache_destroy(pt_cache *c) { delete c; return PT_OK; }
+
+pt_status pt_cache_query_device(pt_cache *c, const pt_cache_query *queries, size_t count, float *rgb, void *stream) {
+    return guard([&]() {
+        if (!c || (count && (!queries || !rgb))) throw Error(PT_INVALID_ARGUMENT, "null argument");
+        if (!count) return;
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        size_t tiles = (count + kTile - 1) / kTile;
+        int grid = int(std::min<size_t>(tiles, size_t(2 * c->ctas)));
+        float3 lo = make_float3(c->lo[0], c->lo[1], c->lo[2]), hi = make_float3(c->hi[0], c->hi[1], c->hi[2]);
+        forward_kernel<<<grid, kTile, kFwdSmem, st>>>(c->weights.get<unsigned char>(), queries, count, lo, hi, rgb, c->status.get<int>());
+        PT_CUDA(cudaGetLastError());
+    });
+}
+
+pt_status pt_cache_gradients(pt_cache *c, const pt_cache_query *queries, const float *targets, size_t count, float *grad_host,
+                             float *loss) {
+    return guard([&]() {
+        if (!c || !queries || !targets || !count) throw Error(PT_INVALID_ARGUMENT, "invalid gradient arguments");
+        float l = gradients(c, queries, targets, count, nullptr);
+        if (loss) *loss = l / float(count * kOut);
+        if (grad_host) PT_CUDA(cudaMemcpy(grad_host, c->grad.get(), kMasterFloats * sizeof(float), cudaMemcpyDeviceToHost));
+    });
+}
+
+pt_status pt_cache_train_device(pt_cache *c, const pt_cache_query *queries, const float *targets, size_t count, float *loss,
+                                void *stream) {
+    return guard([&]() {
+        if (!c || !queries || !targets || !count) throw Error(PT_INVALID_ARGUMENT, "invalid training arguments");
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        float l = gradients(c, queries, targets, count, st);
+        c->step++;
+        adam_kernel<<<(kMasterFloats + 255) / 256, 256, 0, st>>>(c->master.get<float>(), c->adam_m.get<float>(), c->adam_v.get<float>(),
+                                                                 c->grad.get<float>(), c->step, c->lr, c->beta1, c->beta2, c->eps,
+                                                                 c->weights.get<unsigned char>());
+        PT_CUDA(cudaGetLastError());
+        if (loss) *loss = l / float(count * kOut);
+    });
+}
+
+pt_status pt_cache_weights(pt_cache *c, float *get, const float *set, size_t floats) {
+    return guard([&]() {
+        if (!c || floats != size_t(kMasterFloats)) throw Error(PT_INVALID_ARGUMENT, "weights hold 20672 floats");
+        if (get) PT_CUDA(cudaMemcpy(get, c->master.get(), floats * sizeof(float), cudaMemcpyDeviceToHost));
+        if (set) {
+            PT_CUDA(cudaMemcpy(c->master.get(), set, floats * sizeof(float), cudaMemcpyHostToDevice));
+            refresh_canon(c, nullptr);
+            PT_CUDA(cudaDeviceSynchronize());
+        }
+    });
+}
+
+pt_status pt_cache_hyper(pt_cache *c, float lr, float beta1, float beta2, float eps) {
+    return guard([&]() {
+        if (!c || !(lr > 0) || !(beta1 >= 0 && beta1 < 1) || !(beta2 >= 0 && beta2 < 1) || !(eps > 0))
+            throw Error(PT_INVALID_ARGUMENT, "invalid Adam settings");
+        c->lr = lr; c->beta1 = beta1; c->beta2 = beta2; c->eps = eps;
+    });
+}
+
+} // extern "C"

@@ -148,6 +148,13 @@ def library() -> C.CDLL:
         "pt_batch_stats": (I, [P, P, P, P, S]),
         "pt_batch_tuning": (I, [P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
         "pt_batch_autotune": (I, [P, C.c_int32, C.c_char_p, P]),
+        "pt_cache_create": (I, [P, P, U64, P]),
+        "pt_cache_destroy": (I, [P]),
+        "pt_cache_query_device": (I, [P, P, S, P, P]),
+        "pt_cache_train_device": (I, [P, P, P, S, P, P]),
+        "pt_cache_gradients": (I, [P, P, P, S, P, P]),
+        "pt_cache_weights": (I, [P, P, P, S]),
+        "pt_cache_hyper": (I, [P, F, F, F, F]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -569,3 +576,58 @@ class Batch:
         done = np.zeros(len(self.jobs), np.float64)
         check(library().pt_batch_stats(self._h, C.byref(ms), C.byref(rays), done.ctypes.data, len(done)))
         return ms.value, rays.value, done
+
+
+# ---------------------------------------------------------------- radiance cache
+CACHE_QUERY = np.dtype([("position", *VEC3), ("direction", *VEC3), ("normal", *VEC3), ("albedo", *VEC3),
+                        ("roughness", "<f4")])
+assert CACHE_QUERY.itemsize == 52
+CACHE_WEIGHTS = 20672
+
+
+class RadianceCache:
+    """The tcgen05 radiance-cache MLP (pt_cache_*).  Query/train take device addresses or torch
+    tensors (queries: CACHE_QUERY records, targets/outputs: 3 floats per query)."""
+
+    def __init__(self, scene_lo, scene_hi, seed: int = 1):
+        self._h = C.c_void_p()
+        lo = (C.c_float * 3)(*scene_lo)
+        hi = (C.c_float * 3)(*scene_hi)
+        check(library().pt_cache_create(lo, hi, seed, C.byref(self._h)))
+
+    def close(self):
+        if self._h:
+            library().pt_cache_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def query(self, queries, count: int, out, stream=0) -> None:
+        check(library().pt_cache_query_device(self._h, _ptr(queries), count, _ptr(out), stream))
+
+    def train(self, queries, targets, count: int, stream=0) -> float:
+        loss = C.c_float()
+        check(library().pt_cache_train_device(self._h, _ptr(queries), _ptr(targets), count, C.byref(loss), stream))
+        return loss.value
+
+    def gradients(self, queries, targets, count: int):
+        g = np.zeros(CACHE_WEIGHTS, np.float32)
+        loss = C.c_float()
+        check(library().pt_cache_gradients(self._h, _ptr(queries), _ptr(targets), count, g.ctypes.data, C.byref(loss)))
+        return loss.value, g
+
+    def weights(self) -> np.ndarray:
+        w = np.zeros(CACHE_WEIGHTS, np.float32)
+        check(library().pt_cache_weights(self._h, w.ctypes.data, None, CACHE_WEIGHTS))
+        return w
+
+    def set_weights(self, w: np.ndarray) -> None:
+        w = np.ascontiguousarray(w, np.float32)
+        check(library().pt_cache_weights(self._h, None, w.ctypes.data, CACHE_WEIGHTS))
+
+    def hyper(self, lr=1e-2, beta1=0.9, beta2=0.99, eps=1e-8) -> None:
+        check(library().pt_cache_hyper(self._h, lr, beta1, beta2, eps))

@@ -247,6 +247,32 @@ pt_status pt_batch_tuning(pt_batch *batch, int32_t path_capacity, int32_t block,
  * `cache_path` (NULL: no cache).  best = {capacity, block, min_active, use_graph}. */
 pt_status pt_batch_autotune(pt_batch *batch, int32_t probe_samples, const char *cache_path, int32_t *best);
 
+/* ---- learned radiance cache ----
+ * A small MLP (64 encoded inputs -> 5 hidden layers of 64, ReLU -> 3 outputs, exp) trained
+ * online on radiance samples and queried for the outgoing radiance at a path vertex.  Forward
+ * and backward run on the tensor cores (tcgen05, BF16 operands, FP32 accumulation in TMEM);
+ * Adam updates FP32 master weights.  Inputs: position (frequency-encoded over the scene box, 3 x
+ * 12), direction (spherical harmonics up to degree 3, 16), normal, albedo, roughness (7).
+ * Loss: relative L2, mean over samples and channels of (y - t)^2 / (y^2 + 0.01) with y treated
+ * as a constant in the denominator.  No counterpart in the reference. */
+typedef struct pt_cache_query { pt_vec3 position, direction, normal, albedo; float roughness; } pt_cache_query;
+typedef struct pt_cache pt_cache;
+#define PT_CACHE_WEIGHTS 20672   /* FP32 masters: W0..W4 (64 x 64, [in][out]) then W5 (64 x 3) */
+pt_status pt_cache_create(const float scene_lo[3], const float scene_hi[3], uint64_t seed, pt_cache **out);
+pt_status pt_cache_destroy(pt_cache *cache);
+/* rgb[3 * i] = prediction for queries[i]; device buffers, asynchronous on `stream`. */
+pt_status pt_cache_query_device(pt_cache *cache, const pt_cache_query *queries, size_t count, float *rgb, void *stream);
+/* One Adam step on (queries, targets) (device buffers); *loss = the batch's mean loss (host). */
+pt_status pt_cache_train_device(pt_cache *cache, const pt_cache_query *queries, const float *targets, size_t count,
+                                float *loss, void *stream);
+/* The gradient of the mean loss w.r.t. the FP32 masters (host buffer of PT_CACHE_WEIGHTS), no update. */
+pt_status pt_cache_gradients(pt_cache *cache, const pt_cache_query *queries, const float *targets, size_t count,
+                             float *grad, float *loss);
+/* Reads (get != NULL) and/or replaces (set != NULL) the FP32 master weights. */
+pt_status pt_cache_weights(pt_cache *cache, float *get, const float *set, size_t floats);
+/* Adam hyper-parameters (defaults 1e-2, 0.9, 0.99, 1e-8). */
+pt_status pt_cache_hyper(pt_cache *cache, float lr, float beta1, float beta2, float eps);
+
 #ifdef __cplusplus
 }
 #endif
