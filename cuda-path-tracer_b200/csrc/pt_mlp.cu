@@ -236,7 +236,8 @@ struct Sync {
 constexpr size_t kFwdSmem = 256 + kWeightBytes + kPad + 2 * (kActBytes + kPad);
 
 __global__ void __launch_bounds__(kTile, 1) forward_kernel(const unsigned char *weights, const pt_cache_query *queries, size_t count,
-                                                           float3 lo, float3 hi, float *out, int *status) {
+                                                           const int32_t *count_dev, float3 lo, float3 hi, float *out, int *status) {
+    if (count_dev) count = min(count, size_t(max(0, *count_dev)));   // queue length known only on the device
     extern __shared__ __align__(1024) unsigned char smem[];
     Scratch *h = reinterpret_cast<Scratch *>(smem);
     unsigned char *w = smem + 256;
@@ -305,8 +306,10 @@ __global__ void __launch_bounds__(kTile, 1) forward_kernel(const unsigned char *
 constexpr size_t kTrainSmem = 256 + kWeightBytes + kPad + 6 * (kActBytes + kPad) + (kActBytes + kPad) + (kOutActBytes + kPad);
 
 __global__ void __launch_bounds__(kTile, 1) train_kernel(const unsigned char *weights, const pt_cache_query *queries,
-                                                         const float *targets, size_t count, float3 lo, float3 hi,
-                                                         float grad_scale, float *partial, float *loss_partial, int *status) {
+                                                         const float *targets, size_t count, const int32_t *count_dev,
+                                                         float3 lo, float3 hi, float *partial, float *loss_partial, int *status) {
+    if (count_dev) count = min(count, size_t(max(0, *count_dev)));
+    const float grad_scale = count ? 1.0f / float(count * kOut) : 0.0f;   // mean over samples and channels
     extern __shared__ __align__(1024) unsigned char smem[];
     Scratch *h = reinterpret_cast<Scratch *>(smem);
     unsigned char *w = smem + 256;
@@ -435,9 +438,19 @@ __global__ void __launch_bounds__(kTile, 1) train_kernel(const unsigned char *we
     tmem_free(tbase, 512);
 }
 
-// Sums the per-CTA partials in a fixed order (deterministic) into `grad`.
-__global__ void reduce_kernel(const float *partial, int ctas, float *grad) {
+// Sums the per-CTA partials in a fixed order (deterministic) into `grad`; thread 0 also sums the
+// loss partials into loss[0] (mean) and, for a training step (advance) on a non-empty batch,
+// advances the Adam step (step[0]) and the weight-average step (step[1]).
+__global__ void reduce_kernel(const float *partial, const float *loss_partial, int ctas, size_t count, const int32_t *count_dev,
+                              float *grad, float *loss, int *step, int advance) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) {
+        size_t n = count_dev ? min(count, size_t(max(0, *count_dev))) : count;
+        float l = 0.0f;
+        for (int c = 0; c < ctas; c++) l += loss_partial[c];
+        loss[0] = n ? l / float(n * kOut) : 0.0f;
+        if (n && advance) { step[0] += 1; step[1] += 1; }
+    }
     if (i >= kMasterFloats) return;
     float s = 0.0f;
     for (int c = 0; c < ctas; c++) s += partial[size_t(c) * kMasterFloats + i];
@@ -455,10 +468,16 @@ __host__ __device__ inline uint32_t master_to_canon(int i) {
 }
 
 // Adam (bias-corrected) on the FP32 masters; writes the bf16 canonical copy.
-__global__ void adam_kernel(float *master, float *m, float *v, const float *grad, int step, float lr, float beta1, float beta2,
-                            float eps, unsigned char *canon_out) {
+// The step count lives on the device so that a captured graph replays with the right bias
+// correction; an empty batch (count_dev == 0) leaves the weights alone.  With ema_decay > 0 the
+// kernel also keeps the exponential moving average of the weights (bias-corrected, as Adam's
+// moments are) and writes its bf16 copy, the weights that inference uses.
+__global__ void adam_kernel(float *master, float *m, float *v, const float *grad, const int *step_dev, const int32_t *count_dev,
+                            float lr, float beta1, float beta2, float eps, unsigned char *canon_out, float ema_decay,
+                            float *ema, unsigned char *ema_canon) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= kMasterFloats) return;
+    if (i >= kMasterFloats || (count_dev && *count_dev <= 0)) return;
+    const int step = step_dev[0];
     float g = grad[i];
     float mi = beta1 * m[i] + (1.0f - beta1) * g;
     float vi = beta2 * v[i] + (1.0f - beta2) * g * g;
@@ -466,7 +485,14 @@ __global__ void adam_kernel(float *master, float *m, float *v, const float *grad
     float mh = mi / (1.0f - powf(beta1, float(step))), vh = vi / (1.0f - powf(beta2, float(step)));
     float w = master[i] - lr * mh / (sqrtf(vh) + eps);
     master[i] = w;
-    *reinterpret_cast<__nv_bfloat16 *>(canon_out + master_to_canon(i)) = __float2bfloat16_rn(w);
+    const uint32_t at = master_to_canon(i);
+    *reinterpret_cast<__nv_bfloat16 *>(canon_out + at) = __float2bfloat16_rn(w);
+    if (ema_decay > 0.0f) {
+        float e = ema_decay * ema[i] + (1.0f - ema_decay) * w;
+        ema[i] = e;
+        float corrected = e / (1.0f - powf(ema_decay, float(step_dev[1])));
+        *reinterpret_cast<__nv_bfloat16 *>(ema_canon + at) = __float2bfloat16_rn(corrected);
+    }
 }
 
 __global__ void canon_kernel(const float *master, unsigned char *canon_out) {
@@ -481,17 +507,23 @@ __global__ void canon_kernel(const float *master, unsigned char *canon_out) {
 using namespace ptb::mlp;
 
 struct pt_cache {
-    DeviceBuffer master, adam_m, adam_v, grad, weights, partial, loss_partial, status;
+    DeviceBuffer master, adam_m, adam_v, grad, weights, partial, loss_partial, status, step, loss;
+    DeviceBuffer ema, ema_weights;      // weight average and its bf16 copy (used for inference when ema_decay > 0)
     float lo[3], hi[3];
-    int step = 0;
     int ctas = 0;
     float lr = 1e-2f, beta1 = 0.9f, beta2 = 0.99f, eps = 1e-8f;
+    float ema_decay = 0.0f;
+    const unsigned char *inference() const { return (ema_decay > 0 ? ema_weights : weights).get<unsigned char>(); }
 };
 
 namespace {
+// bf16 copies from the masters; the weight average restarts from them (step[1] = 0)
 void refresh_canon(pt_cache *c, cudaStream_t st) {
     canon_kernel<<<(kMasterFloats + 255) / 256, 256, 0, st>>>(c->master.get<float>(), c->weights.get<unsigned char>());
     PT_CUDA(cudaGetLastError());
+    PT_CUDA(cudaMemcpyAsync(c->ema_weights.get(), c->weights.get(), kWeightBytes, cudaMemcpyDeviceToDevice, st));
+    PT_CUDA(cudaMemsetAsync(c->ema.get(), 0, kMasterFloats * sizeof(float), st));
+    PT_CUDA(cudaMemsetAsync(c->step.get<int>() + 1, 0, sizeof(int), st));
 }
 void check_status(pt_cache *c) {
     int status = 0;
@@ -501,29 +533,55 @@ void check_status(pt_cache *c) {
         throw Error(pt_status(status), "radiance-cache kernel timed out waiting for the tensor cores");
     }
 }
-int train_grid(pt_cache *c, size_t count) {
+float3 lo3(const pt_cache *c) { return make_float3(c->lo[0], c->lo[1], c->lo[2]); }
+float3 hi3(const pt_cache *c) { return make_float3(c->hi[0], c->hi[1], c->hi[2]); }
+// forward/backward/reduce into c->grad and c->loss; no host synchronisation
+void gradients(pt_cache *c, const pt_cache_query *q, const float *targets, size_t count, const int32_t *count_dev, bool advance,
+               cudaStream_t st) {
     size_t tiles = (count + kTile - 1) / kTile;
-    return int(std::min<size_t>(tiles ? tiles : 1, size_t(c->ctas)));
-}
-// forward/backward/reduce into c->grad; returns the summed loss
-float gradients(pt_cache *c, const pt_cache_query *q, const float *targets, size_t count, cudaStream_t st) {
-    int grid = train_grid(c, count);
-    float3 lo = make_float3(c->lo[0], c->lo[1], c->lo[2]), hi = make_float3(c->hi[0], c->hi[1], c->hi[2]);
-    float scale = 1.0f / float(count * kOut);
-    train_kernel<<<grid, kTile, kTrainSmem, st>>>(c->weights.get<unsigned char>(), q, targets, count, lo, hi, scale,
+    int grid = count_dev ? c->ctas : int(std::min<size_t>(tiles ? tiles : 1, size_t(c->ctas)));
+    train_kernel<<<grid, kTile, kTrainSmem, st>>>(c->weights.get<unsigned char>(), q, targets, count, count_dev, lo3(c), hi3(c),
                                                    c->partial.get<float>(), c->loss_partial.get<float>(), c->status.get<int>());
     PT_CUDA(cudaGetLastError());
-    reduce_kernel<<<(kMasterFloats + 255) / 256, 256, 0, st>>>(c->partial.get<float>(), grid, c->grad.get<float>());
+    reduce_kernel<<<(kMasterFloats + 255) / 256, 256, 0, st>>>(c->partial.get<float>(), c->loss_partial.get<float>(), grid, count,
+                                                               count_dev, c->grad.get<float>(), c->loss.get<float>(), c->step.get<int>(),
+                                                               advance ? 1 : 0);
     PT_CUDA(cudaGetLastError());
-    std::vector<float> losses(static_cast<size_t>(grid));
-    PT_CUDA(cudaMemcpyAsync(losses.data(), c->loss_partial.get(), losses.size() * sizeof(float), cudaMemcpyDeviceToHost, st));
+}
+float read_loss(pt_cache *c, cudaStream_t st) {
+    float l = 0;
+    PT_CUDA(cudaMemcpyAsync(&l, c->loss.get(), sizeof l, cudaMemcpyDeviceToHost, st));
     PT_CUDA(cudaStreamSynchronize(st));
     check_status(c);
-    double sum = 0;
-    for (float v : losses) sum += v;
-    return float(sum);
+    return l;
 }
 } // namespace
+
+namespace ptb {
+void cache_bounds(const pt_cache *c, float lo[3], float hi[3]) {
+    for (int a = 0; a < 3; a++) { lo[a] = c->lo[a]; hi[a] = c->hi[a]; }
+}
+void cache_forward(pt_cache *c, const pt_cache_query *queries, size_t count, const int32_t *count_dev, float *rgb, cudaStream_t st) {
+    size_t tiles = (count + kTile - 1) / kTile;
+    if (!tiles) return;
+    int grid = int(std::min<size_t>(tiles, size_t(2 * c->ctas)));
+    forward_kernel<<<grid, kTile, kFwdSmem, st>>>(c->inference(), queries, count, count_dev, lo3(c), hi3(c), rgb,
+                                                   c->status.get<int>());
+    PT_CUDA(cudaGetLastError());
+}
+void cache_train(pt_cache *c, const pt_cache_query *queries, const float *targets, size_t count, const int32_t *count_dev,
+                 cudaStream_t st) {
+    if (!count) return;
+    gradients(c, queries, targets, count, count_dev, true, st);
+    adam_kernel<<<(kMasterFloats + 255) / 256, 256, 0, st>>>(c->master.get<float>(), c->adam_m.get<float>(), c->adam_v.get<float>(),
+                                                             c->grad.get<float>(), c->step.get<int>(), count_dev, c->lr, c->beta1,
+                                                             c->beta2, c->eps, c->weights.get<unsigned char>(), c->ema_decay,
+                                                             c->ema.get<float>(), c->ema_weights.get<unsigned char>());
+    PT_CUDA(cudaGetLastError());
+}
+float cache_loss(pt_cache *c, cudaStream_t st) { return read_loss(c, st); }
+void cache_status(pt_cache *c) { check_status(c); }
+} // namespace ptb
 
 extern "C" {
 
@@ -554,11 +612,18 @@ pt_status pt_cache_create(const float scene_lo[3], const float scene_hi[3], uint
             c->adam_m.upload(zeros); c->adam_v.upload(zeros); c->grad.upload(zeros);
             c->weights.resize(kWeightBytes);
             PT_CUDA(cudaMemset(c->weights.get(), 0, kWeightBytes));
+            c->ema_weights.resize(kWeightBytes);
+            PT_CUDA(cudaMemset(c->ema_weights.get(), 0, kWeightBytes));
+            c->ema.resize(kMasterFloats * sizeof(float));
             c->ctas = device_sm_count();
             c->partial.resize(size_t(c->ctas) * kMasterFloats * sizeof(float));
             c->loss_partial.resize(size_t(c->ctas) * sizeof(float));
             c->status.resize(sizeof(int));
             PT_CUDA(cudaMemset(c->status.get(), 0, sizeof(int)));
+            c->step.resize(2 * sizeof(int));
+            PT_CUDA(cudaMemset(c->step.get(), 0, 2 * sizeof(int)));
+            c->loss.resize(sizeof(float));
+            PT_CUDA(cudaMemset(c->loss.get(), 0, sizeof(float)));
             PT_CUDA(cudaFuncSetAttribute(forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kFwdSmem)));
             PT_CUDA(cudaFuncSetAttribute(train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kTrainSmem)));
             refresh_canon(c, nullptr);
@@ -574,12 +639,7 @@ pt_status pt_cache_query_device(pt_cache *c, const pt_cache_query *queries, size
     return guard([&]() {
         if (!c || (count && (!queries || !rgb))) throw Error(PT_INVALID_ARGUMENT, "null argument");
         if (!count) return;
-        cudaStream_t st = static_cast<cudaStream_t>(stream);
-        size_t tiles = (count + kTile - 1) / kTile;
-        int grid = int(std::min<size_t>(tiles, size_t(2 * c->ctas)));
-        float3 lo = make_float3(c->lo[0], c->lo[1], c->lo[2]), hi = make_float3(c->hi[0], c->hi[1], c->hi[2]);
-        forward_kernel<<<grid, kTile, kFwdSmem, st>>>(c->weights.get<unsigned char>(), queries, count, lo, hi, rgb, c->status.get<int>());
-        PT_CUDA(cudaGetLastError());
+        cache_forward(c, queries, count, nullptr, rgb, static_cast<cudaStream_t>(stream));
     });
 }
 
@@ -587,8 +647,9 @@ pt_status pt_cache_gradients(pt_cache *c, const pt_cache_query *queries, const f
                              float *loss) {
     return guard([&]() {
         if (!c || !queries || !targets || !count) throw Error(PT_INVALID_ARGUMENT, "invalid gradient arguments");
-        float l = gradients(c, queries, targets, count, nullptr);
-        if (loss) *loss = l / float(count * kOut);
+        gradients(c, queries, targets, count, nullptr, false, nullptr);
+        float l = read_loss(c, nullptr);
+        if (loss) *loss = l;
         if (grad_host) PT_CUDA(cudaMemcpy(grad_host, c->grad.get(), kMasterFloats * sizeof(float), cudaMemcpyDeviceToHost));
     });
 }
@@ -598,13 +659,8 @@ pt_status pt_cache_train_device(pt_cache *c, const pt_cache_query *queries, cons
     return guard([&]() {
         if (!c || !queries || !targets || !count) throw Error(PT_INVALID_ARGUMENT, "invalid training arguments");
         cudaStream_t st = static_cast<cudaStream_t>(stream);
-        float l = gradients(c, queries, targets, count, st);
-        c->step++;
-        adam_kernel<<<(kMasterFloats + 255) / 256, 256, 0, st>>>(c->master.get<float>(), c->adam_m.get<float>(), c->adam_v.get<float>(),
-                                                                 c->grad.get<float>(), c->step, c->lr, c->beta1, c->beta2, c->eps,
-                                                                 c->weights.get<unsigned char>());
-        PT_CUDA(cudaGetLastError());
-        if (loss) *loss = l / float(count * kOut);
+        cache_train(c, queries, targets, count, nullptr, st);
+        if (loss) *loss = read_loss(c, st);
     });
 }
 
@@ -617,6 +673,17 @@ pt_status pt_cache_weights(pt_cache *c, float *get, const float *set, size_t flo
             refresh_canon(c, nullptr);
             PT_CUDA(cudaDeviceSynchronize());
         }
+    });
+}
+
+pt_status pt_cache_average(pt_cache *c, float decay) {
+    return guard([&]() {
+        if (!c || !(decay >= 0 && decay < 1)) throw Error(PT_INVALID_ARGUMENT, "weight-average decay must be in [0, 1)");
+        c->ema_decay = decay;
+        PT_CUDA(cudaMemcpy(c->ema_weights.get(), c->weights.get(), kWeightBytes, cudaMemcpyDeviceToDevice));
+        PT_CUDA(cudaMemset(c->ema.get(), 0, kMasterFloats * sizeof(float)));
+        PT_CUDA(cudaMemset(c->step.get<int>() + 1, 0, sizeof(int)));
+        PT_CUDA(cudaDeviceSynchronize());
     });
 }
 

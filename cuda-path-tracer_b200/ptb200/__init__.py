@@ -155,6 +155,15 @@ def library() -> C.CDLL:
         "pt_cache_gradients": (I, [P, P, P, S, P, P]),
         "pt_cache_weights": (I, [P, P, P, S]),
         "pt_cache_hyper": (I, [P, F, F, F, F]),
+        "pt_cache_average": (I, [P, F]),
+        "pt_cached_defaults": (I, [P]),
+        "pt_cached_create": (I, [P, P, C.c_int, C.c_int, U64, C.c_int, P, P]),
+        "pt_cached_destroy": (I, [P]),
+        "pt_cached_frames": (I, [P, C.c_int, C.c_int]),
+        "pt_cached_clear": (I, [P]),
+        "pt_cached_get_sums": (I, [P, P, S]),
+        "pt_cached_stats": (I, [P, P, P, P, P, P, P]),
+        "pt_cached_cache": (I, [P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -591,12 +600,21 @@ class RadianceCache:
 
     def __init__(self, scene_lo, scene_hi, seed: int = 1):
         self._h = C.c_void_p()
+        self._owner = None
         lo = (C.c_float * 3)(*scene_lo)
         hi = (C.c_float * 3)(*scene_hi)
         check(library().pt_cache_create(lo, hi, seed, C.byref(self._h)))
 
+    @classmethod
+    def _borrowed(cls, handle, owner):
+        """A view of a network another object owns (kept alive through `owner`)."""
+        self = cls.__new__(cls)
+        self._h = handle
+        self._owner = owner
+        return self
+
     def close(self):
-        if self._h:
+        if self._h and self._owner is None:
             library().pt_cache_destroy(self._h)
             self._h = C.c_void_p()
 
@@ -631,3 +649,84 @@ class RadianceCache:
 
     def hyper(self, lr=1e-2, beta1=0.9, beta2=0.99, eps=1e-8) -> None:
         check(library().pt_cache_hyper(self._h, lr, beta1, beta2, eps))
+
+    def average(self, decay: float) -> None:
+        """Queries use a bias-corrected moving average of the weights (decay 0: the weights)."""
+        check(library().pt_cache_average(self._h, decay))
+
+
+class CachedParams(C.Structure):
+    """pt_cached_params (include/pt.h)."""
+    _fields_ = [("training_paths", C.c_int32), ("train_steps", C.c_int32), ("suffix_bounces", C.c_int32),
+                ("use_cache", C.c_int32), ("train", C.c_int32), ("use_graph", C.c_int32),
+                ("spread_threshold", C.c_float), ("learning_rate", C.c_float), ("network_seed", C.c_uint64),
+                ("wavefront_iterations", C.c_int32), ("query_specular", C.c_int32),
+                ("weight_average", C.c_float), ("reserved", C.c_int32)]
+
+
+class CachedRenderer:
+    """Path tracing with the learned radiance cache (pt_cached_*): frames of one sample per pixel,
+    paths ended at the tcgen05 network after their first wide diffuse bounce, the network trained
+    online on the renderer's own training paths.  ``use_cache=False`` is the plain path tracer
+    through the same kernels.  No counterpart in the reference."""
+
+    def __init__(self, scene, camera: np.ndarray, width: int, height: int, seed: int = 1, max_depth: int = 12, **params):
+        self.scene = scene if isinstance(scene, Scene) else Scene(scene)
+        self.width, self.height = width, height
+        p = CachedParams()
+        check(library().pt_cached_defaults(C.byref(p)))
+        for k, v in params.items():
+            if k not in dict(CachedParams._fields_):
+                raise TypeError(f"unknown radiance-cache setting {k!r}")
+            setattr(p, k, int(v) if isinstance(v, bool) else v)
+        self.params = p
+        self._camera = np.ascontiguousarray(camera, CAMERA)
+        self._h = C.c_void_p()
+        check(library().pt_cached_create(self.scene.handle, self._camera.ctypes.data, width, height, seed, max_depth,
+                                         C.byref(p), C.byref(self._h)))
+
+    def close(self):
+        if self._h:
+            library().pt_cached_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def frames(self, count: int, accumulate: bool = True) -> None:
+        check(library().pt_cached_frames(self._h, count, int(accumulate)))
+
+    def train(self, count: int) -> None:
+        """Training-only frames: only the training paths are traced; the image is left alone."""
+        self.frames(count, accumulate=False)
+
+    def clear(self) -> None:
+        check(library().pt_cached_clear(self._h))
+
+    def sums(self) -> np.ndarray:
+        out = np.zeros((self.height, self.width, 3), np.float32)
+        check(library().pt_cached_get_sums(self._h, out.ctypes.data, out.size))
+        return out
+
+    def image(self) -> np.ndarray:
+        """Mean radiance per pixel over the accumulated frames (float64)."""
+        n = self.stats()["frames"]
+        return self.sums().astype(np.float64) / max(n, 1)
+
+    def stats(self) -> dict:
+        frames = C.c_int()
+        ms = C.c_float()
+        rays, queries, samples = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        loss = C.c_float()
+        check(library().pt_cached_stats(self._h, C.byref(frames), C.byref(ms), C.byref(rays), C.byref(queries),
+                                        C.byref(samples), C.byref(loss)))
+        return dict(frames=frames.value, kernel_ms=ms.value, rays=rays.value, queries=queries.value,
+                    samples=samples.value, loss=loss.value)
+
+    def cache(self) -> RadianceCache:
+        h = C.c_void_p()
+        check(library().pt_cached_cache(self._h, C.byref(h)))
+        return RadianceCache._borrowed(h, self)

@@ -262,7 +262,8 @@ pt_status pt_cache_create(const float scene_lo[3], const float scene_hi[3], uint
 pt_status pt_cache_destroy(pt_cache *cache);
 /* rgb[3 * i] = prediction for queries[i]; device buffers, asynchronous on `stream`. */
 pt_status pt_cache_query_device(pt_cache *cache, const pt_cache_query *queries, size_t count, float *rgb, void *stream);
-/* One Adam step on (queries, targets) (device buffers); *loss = the batch's mean loss (host). */
+/* One Adam step on (queries, targets) (device buffers).  loss == NULL: asynchronous on `stream`;
+ * otherwise the call waits and *loss = the batch's mean loss. */
 pt_status pt_cache_train_device(pt_cache *cache, const pt_cache_query *queries, const float *targets, size_t count,
                                 float *loss, void *stream);
 /* The gradient of the mean loss w.r.t. the FP32 masters (host buffer of PT_CACHE_WEIGHTS), no update. */
@@ -272,6 +273,54 @@ pt_status pt_cache_gradients(pt_cache *cache, const pt_cache_query *queries, con
 pt_status pt_cache_weights(pt_cache *cache, float *get, const float *set, size_t floats);
 /* Adam hyper-parameters (defaults 1e-2, 0.9, 0.99, 1e-8). */
 pt_status pt_cache_hyper(pt_cache *cache, float lr, float beta1, float beta2, float eps);
+/* decay > 0: every Adam step also updates an exponential moving average of the weights
+ * (bias-corrected) and queries use the average; 0 (the default): queries use the weights.
+ * Restarts the average from the current weights. */
+pt_status pt_cache_average(pt_cache *cache, float decay);
+
+/* ---- radiance-cache renderer ----
+ * Renders frames of one sample per pixel with MIS (the shading of the plain renderer) and ends
+ * each path at its first diffuse vertex whose path spread exceeds `spread_threshold` times the
+ * primary footprint (the area-spread heuristic of neural radiance caching): the pixel gets the
+ * path's radiance so far plus throughput x albedo x the network's prediction there.  About
+ * `training_paths` pixels per frame (chosen by a hash of seed, frame and pixel) trace on for
+ * `suffix_bounces` more bounces and end at the cache; the radiance they collect after each
+ * diffuse vertex, divided by its albedo, is a training target, and `train_steps` Adam steps per
+ * frame fit the network to them.  A frame is one CUDA graph launch.  No counterpart in the
+ * reference; use_cache = 0 gives the plain path tracer through the same kernels. */
+typedef struct pt_cached_params {
+    int32_t training_paths;     /* per frame (default 65536) */
+    int32_t train_steps;        /* Adam steps per frame (4); the training samples are split between them */
+    int32_t suffix_bounces;     /* bounces traced beyond the query by training paths (4, at most 8) */
+    int32_t use_cache;          /* 1: end paths at the cache; 0: plain path tracing */
+    int32_t train;              /* 1: online training; 0: the network stays as it is */
+    int32_t use_graph;          /* 1: one graph launch per frame; 0: the same kernels launched one by one */
+    float spread_threshold;     /* c of the termination rule (0.01) */
+    float learning_rate;        /* Adam learning rate (1e-2; beta 0.9 / 0.99) */
+    uint64_t network_seed;      /* weight initialisation */
+    int32_t wavefront_iterations; /* bounces run as wavefront kernels before the fused kernel ends the rest (3) */
+    int32_t query_specular;     /* 0: paths end at diffuse vertices only; 1: also at metal and glass vertices */
+    float weight_average;       /* decay of the weight average queries use (0.99; 0: the live weights) */
+    int32_t reserved;
+} pt_cached_params;
+typedef struct pt_cached_renderer pt_cached_renderer;
+/* params == NULL: the defaults above. */
+pt_status pt_cached_defaults(pt_cached_params *params);
+pt_status pt_cached_create(const pt_scene *scene, const pt_camera *camera, int width, int height, uint64_t seed, int max_depth,
+                           const pt_cached_params *params, pt_cached_renderer **out);
+pt_status pt_cached_destroy(pt_cached_renderer *renderer);
+/* `frames` frames; accumulate = 0: training-only frames (only the training paths are traced and
+ * the image is left alone), 1: every pixel is rendered and added to the image sums. */
+pt_status pt_cached_frames(pt_cached_renderer *renderer, int frames, int accumulate);
+/* Clears the image sums and frame count (the network and the pixels' RNG streams go on). */
+pt_status pt_cached_clear(pt_cached_renderer *renderer);
+pt_status pt_cached_get_sums(const pt_cached_renderer *renderer, float *rgb, size_t floats);
+/* frames: accumulated frames; kernel_ms: device time of all frames; rays: closest-hit + shadow
+ * queries; queries: cache queries; samples: training samples; loss: mean loss of the last step. */
+pt_status pt_cached_stats(pt_cached_renderer *renderer, int *frames, float *kernel_ms, uint64_t *rays, uint64_t *queries,
+                          uint64_t *samples, float *loss);
+/* The renderer's network (owned by the renderer; valid until pt_cached_destroy). */
+pt_status pt_cached_cache(pt_cached_renderer *renderer, pt_cache **cache);
 
 #ifdef __cplusplus
 }

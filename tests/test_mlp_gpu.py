@@ -2,7 +2,8 @@
 
 Bars (BF16 operands, FP32 accumulation): forward outputs within 2e-2 relative; gradients of
 every weight matrix with cosine similarity > 0.999 and relative L2 error < 2e-2; an Adam step
-within 1e-3 relative of the oracle's; training on a smooth target lowers the loss tenfold."""
+within 1e-3 relative of the oracle's; training on a smooth target lowers the loss tenfold; queries
+run on the bias-corrected weight average when one is kept."""
 from __future__ import annotations
 
 import numpy as np
@@ -93,3 +94,34 @@ def test_training_lowers_the_loss():
     for _ in range(300):
         last = cache.train(dq, dt, n)
     assert np.isfinite(last) and last < first / 10, (first, last)
+
+
+def test_weight_average_is_what_queries_use():
+    """With a decay d, queries run on sum_k (1-d) d^(t-k) w_k / (1 - d^t) over the weights after
+    each of the t steps; pt_cache_average restarts the average."""
+    torch = pytest.importorskip("torch")
+    n, d = 2048, 0.9
+    cache = pt.RadianceCache(LO, HI, seed=13)
+    cache.average(d)
+    q = queries(n, 31)
+    t = target_fn(q)
+    dq, dt = to_dev(q), to_dev(t)
+    avg = np.zeros(pt.CACHE_WEIGHTS)
+    for step in range(1, 6):
+        cache.train(dq, dt, n)
+        avg = d * avg + (1 - d) * cache.weights().astype(np.float64)
+    expect_w = (avg / (1 - d ** 5)).astype(np.float32)
+    out = torch.zeros(n * 3, dtype=torch.float32, device="cuda")
+    cache.query(dq, n, out)
+    torch.cuda.synchronize()
+    got = out.cpu().numpy().reshape(n, 3)
+    x = mo.encode(q, LO, HI)
+    want = mo.forward(expect_w, x)
+    assert (np.abs(got - want) / np.maximum(np.abs(want), 1e-6)).max() < 2e-2
+    live = mo.forward(cache.weights(), x)
+    assert np.abs(live - want).max() > 1e-3          # the average is not the live weights
+    cache.average(0.0)                               # queries on the live weights again
+    cache.query(dq, n, out)
+    torch.cuda.synchronize()
+    got = out.cpu().numpy().reshape(n, 3)
+    assert (np.abs(got - live) / np.maximum(np.abs(live), 1e-6)).max() < 2e-2
