@@ -7,6 +7,8 @@ closest hits, with tmin 0.001 and tmax FLT_MAX as cuda_query_rays uses.  Inputs 
 are larger than L2, so no flush is needed between steps.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+  python bench.py --workload batch48      48 render jobs of uneven size in one graph launch
+  python bench.py --workload cache        radiance cache vs plain path tracing, relMSE vs time at 1080p
 
 --impl reference times the reference's own CPU traversal (trace_world on host_view, built from
 its sources into oracle/_ref/) on all host threads over a bounded sample of the same rays.
@@ -46,9 +48,12 @@ def parse():
     ap.add_argument("--log2-rays", type=int, default=LOG2_RAYS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", choices=["query", "batch48"], default="query",
-                    help="query: the closest-hit benchmark (default); batch48: 48 render jobs in one launch")
+    ap.add_argument("--workload", choices=["query", "batch48", "cache"], default="query",
+                    help="query: the closest-hit benchmark (default); batch48: 48 render jobs in one launch; "
+                         "cache: radiance-cache renderer vs plain, time to a relMSE at 1920x1080")
     ap.add_argument("--jobs", type=int, default=48)
+    ap.add_argument("--ref-spp", type=int, default=65536, help="cache workload: samples of the FP64 reference image")
+    ap.add_argument("--max-spp", type=int, default=4096, help="cache workload: sample budget of each curve")
     return ap.parse_args()
 
 
@@ -215,6 +220,198 @@ def run_batch(args):
     print(json.dumps(line), flush=True)
 
 
+def rel_mse_fn(ref: np.ndarray, var_of_mean: np.ndarray):
+    """relMSE = mean over pixels and channels of (x - r)^2 / (r^2 + 1e-2) against the reference r,
+    minus the part the reference's own noise contributes (its per-pixel variance of the mean)."""
+    denom = ref * ref + 1e-2
+    noise = float(np.mean(var_of_mean / denom))
+
+    def rel(x):
+        raw = float(np.mean((x - ref) ** 2 / denom))
+        return raw - noise, raw
+    return rel, noise
+
+
+def crossing(curve, target):
+    """First time (ms) a (samples, ms, relMSE) curve reaches `target`, interpolated log-log
+    between the checkpoints either side; None when it never does."""
+    for k, (n, t, e) in enumerate(curve):
+        if e <= target:
+            if k == 0:
+                return t
+            n0, t0, e0 = curve[k - 1]
+            if e0 <= e or e <= 0:
+                return t
+            f = np.log(e0 / target) / np.log(e0 / e)
+            return float(t0 * (t / t0) ** f)
+    return None
+
+
+def run_cache(args):
+    """Radiance cache vs plain path tracing on the procedural 1M-triangle scene at 1920x1080,
+    depth 12, MIS: relMSE-vs-time curves against an FP64-accumulated plain reference, the time
+    each method needs to reach relMSE <= 1e-3 and the plain method's 1024-spp relMSE, and
+    relMSE at equal time.  Times are device time of the render calls (CUDA events); wall time
+    around the same calls is reported beside them."""
+    import torch
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    W, H, D = 1920, 1080, 12
+    t = time.perf_counter()
+    scene, cam = pt.procedural_scene(W, H)
+    dev = pt.Scene(scene)
+    build_s = time.perf_counter() - t
+    # reference: plain renders of 256 spp with independent seeds, accumulated in float64
+    chunks = max(2, args.ref_spp // 256)
+    acc = np.zeros(W * H * 3)
+    acc2 = np.zeros(W * H * 3)
+    t = time.perf_counter()
+    for k in range(chunks):
+        r = pt.CudaRenderer(dev, cam, W, H, 100000 + k, max_depth=D)
+        r.add_samples(256)
+        m = r.sums().astype(np.float64) / 256
+        acc += m
+        acc2 += m * m
+        r.close()
+    ref = acc / chunks
+    var_of_mean = np.maximum(acc2 / chunks - ref * ref, 0) / (chunks - 1)
+    ref_s = time.perf_counter() - t
+    del acc, acc2
+    rel, noise = rel_mse_fn(ref, var_of_mean)
+    plain_marks = sorted({int(round(8 * 1.25 ** k)) for k in range(60) if 8 * 1.25 ** k <= args.max_spp} | {1024})
+    clocks = Clocks(local)
+    # plain path tracer: the progressive renderer
+    plain = pt.CudaRenderer(dev, cam, W, H, 1, max_depth=D)
+    plain_curve, wall, done = [], 0.0, 0
+    for m in plain_marks:
+        t = time.perf_counter()
+        plain.add_samples(m - done)
+        wall += time.perf_counter() - t
+        done = m
+        e, _ = rel(plain.sums().astype(np.float64) / m)
+        plain_curve.append((m, plain.kernel_milliseconds(), e, wall * 1e3))
+        if e <= 1e-3 and m >= 1024:
+            break
+    plain_rays = plain.rays_traced()
+    plain_1024 = next(c for c in plain_curve if c[0] == 1024)
+    # radiance cache (library defaults), 32 training-only frames first
+    cache = pt.CachedRenderer(dev, cam, W, H, 1, D)
+    spf = cache.params.samples_per_frame
+    t = time.perf_counter()
+    cache.train(32)
+    wall = time.perf_counter() - t
+    cache_curve = []
+    for m in plain_marks:
+        frames = max(0, -(-m // spf) - cache.stats()["frames"] // spf)
+        if frames:
+            t = time.perf_counter()
+            cache.frames(frames)
+            wall += time.perf_counter() - t
+        st = cache.stats()
+        e, _ = rel(cache.sums().astype(np.float64).reshape(-1) / st["frames"])
+        cache_curve.append((st["frames"], st["kernel_ms"], e, wall * 1e3))
+        if e <= 1e-3 and st["kernel_ms"] > plain_1024[1]:
+            break
+    clock = clocks.stop()
+    st = cache.stats()
+    spec = pt.CachedRenderer(dev, cam, W, H, 1, D, query_specular=0, spread_threshold=0.01)   # the diffuse-only rule
+    spec.train(32)
+    spec_curve = []
+    for m in (64, 256, 1024):
+        spec.frames(max(1, (m - spec.stats()["frames"]) // spf))
+        s2 = spec.stats()
+        spec_curve.append((s2["frames"], s2["kernel_ms"], rel(spec.sums().astype(np.float64).reshape(-1) / s2["frames"])[0]))
+    spec.close()
+
+    def pick(curve, target):
+        dev_ms = crossing([(c[0], c[1], c[2]) for c in curve], target)
+        wall_ms = crossing([(c[0], c[3], c[2]) for c in curve], target)
+        return dev_ms, wall_ms
+
+    c_1e3, c_1e3_wall = pick(cache_curve, 1e-3)
+    p_1e3, p_1e3_wall = pick(plain_curve, 1e-3)
+    c_1024, c_1024_wall = pick(cache_curve, plain_1024[2])
+    eq = min(cache_curve, key=lambda c: abs(c[1] - plain_1024[1]))
+    # the MLP kernels alone: forward over 2^21 queries, one training step over 2^16 samples
+    net = cache.cache()
+    nq = 1 << 21
+    q = torch.zeros((nq, 13), dtype=torch.float32, device="cuda")
+    g = torch.Generator(device="cuda").manual_seed(5)
+    q[:, 0:3] = torch.rand(nq, 3, device="cuda", generator=g) * 10
+    q[:, 3:6] = torch.nn.functional.normalize(torch.randn(nq, 3, device="cuda", generator=g), dim=1)
+    q[:, 6:9] = torch.nn.functional.normalize(torch.randn(nq, 3, device="cuda", generator=g), dim=1)
+    q[:, 9:12] = 0.5
+    q[:, 12] = 1.0
+    out = torch.zeros(nq * 3, device="cuda")
+    tgt = torch.rand(nq * 3, device="cuda", generator=g)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn, reps=20):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+    fwd_ms = timed(lambda: net.query(q, nq, out))
+    nt = 1 << 16
+    train_ms = timed(lambda: net.train(q, tgt, nt, wait=False))
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    tpeak = float(peaks.get("bf16_tflops", 1590.0))
+    fwd_tf = 41344.0 * nq / (fwd_ms / 1e3) / 1e12
+    train_tf = 3 * 41344.0 * nt / (train_ms / 1e3) / 1e12
+    # CPU baseline: the reference's host renderer's ray rate on a 960x540 render of the same view,
+    # turned into the time the plain method's rays to relMSE 1e-3 would take on these cores
+    cpu = None
+    sys.path.insert(0, str(ROOT / "oracle"))
+    from oracle_bind import RefCpu, REF_CPU_SO
+    if REF_CPU_SO.exists() and p_1e3 is not None:
+        ref_cpu = RefCpu()
+        threads = os.cpu_count() or 1
+        small, small_cam = pt.procedural_scene(960, 540)
+        t = time.perf_counter()
+        _, _, rays = ref_cpu.render(small, small_cam, 960, 540, 1, [2], nthreads=threads)
+        dt = time.perf_counter() - t
+        rays_to_target = plain_rays / plain_curve[-1][0] * (p_1e3 / plain_curve[-1][1] * plain_curve[-1][0])
+        cpu = {"value": rays_to_target / (rays / dt) * 1e3, "unit": "ms", "cores": threads, "kind": "reference",
+               "sample": f"reference trace_pixel_sample (depth 50) on 960x540 x 2 spp: {rays} rays in {dt:.2f} s "
+                         f"= {rays / dt / 1e6:.1f} Mrays/s; value = plain rays to relMSE 1e-3 at that rate"}
+    line = {
+        "metric": "ms to relMSE<=1e-3 at 1080p (radiance cache)", "value": c_1e3, "unit": "ms", "n_gpus": 1,
+        "steps": st["frames"], "warmup": 32, "ms_per_step": (st["kernel_ms"]) / max(1, st["frames"]),
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "bf16+f32", "data": "synthetic",
+        "config": {"workload": "radiance cache vs plain, procedural 1M-triangle scene, 1920x1080, depth 12, MIS",
+                   "cache": {k: getattr(cache.params, k) for k, _ in pt.CachedParams._fields_},
+                   "reference_image": f"{chunks * 256} spp plain, float64 accumulation", "l2": "frame state > L2"},
+        "plain_ms_to_1e-3": p_1e3, "speedup_to_1e-3": (p_1e3 / c_1e3) if (p_1e3 and c_1e3) else None,
+        "plain_1024spp": {"relmse": plain_1024[2], "ms": plain_1024[1], "cache_ms_to_it": c_1024,
+                          "speedup": (plain_1024[1] / c_1024) if c_1024 else None},
+        "equal_time": {"ms": eq[1], "cache_relmse": eq[2], "plain_relmse_at_1024spp": plain_1024[2]},
+        "wall_ms": {"cache_to_1e-3": c_1e3_wall, "plain_to_1e-3": p_1e3_wall, "cache_to_plain_1024": c_1024_wall},
+        "curves": {"plain": [[c[0], round(c[1], 2), c[2]] for c in plain_curve],
+                   "cache": [[c[0], round(c[1], 2), c[2]] for c in cache_curve],
+                   "cache_diffuse_only_c0.01": [[c[0], round(c[1], 2), c[2]] for c in spec_curve]},
+        "reference": {"spp": chunks * 256, "noise_relmse": noise, "seconds": ref_s},
+        "cache_stats": st,
+        "roofline": {"bound": "tensor", "kernel": "mlp forward", "achieved": fwd_tf, "peak": tpeak, "unit": "TFLOP/s",
+                     "frac": fwd_tf / tpeak, "traffic": None, "peak_kind": "measured" if peaks else "fallback"},
+        "mlp": {"forward_ms_2^21": fwd_ms, "forward_tflops": fwd_tf, "train_step_ms_2^16": train_ms, "train_tflops": train_tf,
+                "flop_per_query": 41344, "flop_per_training_sample": 3 * 41344},
+        "clocks": clock, "scene_build_s": build_s,
+        # per frame: start, 3 per wavefront iteration, the fused tail, forward, resolve, targets,
+        # 3 per Adam step (gradients, reduce, update), frame end
+        "gpu_launches": int((st["frames"] // spf + 32) * (1 + 3 * cache.params.wavefront_iterations + 1 + 3 +
+                                                        3 * cache.params.train_steps + 1)),
+        "e2e": {"value": c_1e3_wall, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": W * H * 12,
+                "api": "pt_cached_frames + pt_cached_get_sums (host wall clock)"},
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -222,6 +419,9 @@ def main():
         return
     if args.workload == "batch48":
         run_batch(args)
+        return
+    if args.workload == "cache":
+        run_cache(args)
         return
     import torch
     import torch.distributed as dist

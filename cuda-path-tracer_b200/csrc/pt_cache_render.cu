@@ -3,13 +3,14 @@
 // No counterpart in the reference (its renderer has no learned component); the shading is the
 // reference's MIS bounce loop (src/renderer/transport.h:169-230) as pt_wavefront.h has it.
 //
-// One frame = one sample per pixel, one path per pixel, run as a wavefront:
+// One frame = `samples_per_frame` samples per pixel, one path per pixel at a time (a pixel's
+// next sample starts when its path ends), run as a wavefront:
 //   start   : camera ray of every pixel (training-only frames: of the training pixels only);
 //             about `training_paths` pixels, picked by a hash of (seed, frame, pixel), also
-//             get a training slot;
+//             get a training slot for their first sample;
 //   extend / shade / shadow, `wavefront_iterations` times, then one fused kernel (a thread per
-//             path) runs the remaining paths to their end (every path ends within max_depth + 1
-//             bounces):
+//             path) runs the remaining paths to their end (a pixel's samples end within
+//             samples_per_frame * (max_depth + 1) bounces):
 //             shade does the MIS step, tracks the path's area spread
 //               a0 = |x0 - x1|^2 / (4 pi cos1),  sqrt(a) += sqrt(|x_{i-1} - x_i|^2 / (pdf_{i-1} cos_i)),
 //             and at the first diffuse vertex (past the primary hit) where a > c * a0 it ends the
@@ -18,7 +19,8 @@
 //             `suffix_bounces` bounces (features, suffix radiance S and suffix throughput U as
 //             seen there), and ends with a cache query at the vertex after them (self-training);
 //   forward : the network on every query of the frame (tcgen05, pt_mlp.cu);
-//   resolve : pixel sums += radiance + weight * prediction for the paths that ended at a query;
+//   resolve : pixel sums += weight * prediction of each of the pixel's queries (in sample order;
+//             the radiance before the query was added when the sample ended);
 //   targets : for each recorded vertex, L = (S_end + U_end * albedo_tail * prediction - S_v) / U_v
 //             is the outgoing radiance there; the sample (features, L / albedo) goes to one of
 //             `train_steps` batches;
@@ -28,6 +30,7 @@
 #include <cfloat>
 #include <algorithm>
 #include <cmath>
+#include <vector>
 #include "pt_api_common.h"
 #include "pt_cache_internal.h"
 #include "pt_device.h"
@@ -54,7 +57,7 @@ struct alignas(16) CachePath {
     int32_t train;                      // training slot, -1: none
     int32_t vertices;                   // training vertices recorded, -1: the query vertex not reached yet
     int32_t qdepth;                     // depth of the query vertex
-    int32_t pad;
+    int32_t samples_left;               // this one included
 };
 static_assert(sizeof(CachePath) == 112, "path record");
 
@@ -85,11 +88,13 @@ struct Params {
     pt_camera camera;
     int width, height, max_depth, wide;
     int use_cache, suffix_bounces, steps, accumulate, wavefront, query_specular;
+    int spf;                            // samples per pixel in this frame
     float spread_c;
     uint32_t train_threshold;           // a pixel trains when its hash is below this
     int32_t train_capacity;             // training slots
     int32_t bucket_capacity;            // samples per Adam step
     uint64_t seed;
+    float radiance_max[3];              // brightest emitted radiance per channel: bounds every L / albedo
 };
 
 struct Buffers {
@@ -108,6 +113,8 @@ struct Buffers {
     pt_cache_query *queries;
     QueryAux *aux;
     float *pred;
+    int32_t *pixel_queries;             // pixel i's queries of the frame, in sample order: [i * spf + j]
+    int32_t *pixel_query_count;
     TrainVertex *vertices;
     TrainEnd *ends;
     pt_cache_query *samples;            // steps x bucket_capacity
@@ -133,6 +140,22 @@ __device__ inline int32_t append(bool take, int32_t *counter) {
     return take ? base + __popc(m & ((1u << lane_id()) - 1u)) : -1;
 }
 
+// A fresh camera sample of pixel i (trace_pixel_sample's camera step, transport.h:232-239).
+__device__ inline void camera_sample(const Params &p, int32_t i, Pcg &rng, int32_t train, int32_t samples_left, CachePath &s) {
+    int x = i % p.width, y = i / p.width;
+    float u = (x + rng.uniform()) / float(p.width);
+    float v = (y + rng.uniform()) / float(p.height);
+    pt_ray r;
+    camera_ray(p.camera, u, v, rng, r);
+    s.ox = r.origin.x; s.oy = r.origin.y; s.oz = r.origin.z; s.time = r.time;
+    s.dx = r.direction.x; s.dy = r.direction.y; s.dz = r.direction.z; s.bounce_pdf = 0;
+    s.tr = 1; s.tg = 1; s.tb = 1; s.prev_pdf = 0;
+    s.rr = 0; s.rg = 0; s.rb = 0; s.spread = 0;
+    s.ur = 1; s.ug = 1; s.ub = 1; s.a0 = 0;
+    s.sr = 0; s.sg = 0; s.sb = 0; s.depth = 0;
+    s.train = train; s.vertices = -1; s.qdepth = 0; s.samples_left = samples_left;
+}
+
 __global__ void start_kernel(Params p, Buffers b, int32_t pixels) {
     const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = i < pixels;
@@ -143,23 +166,22 @@ __global__ void start_kernel(Params p, Buffers b, int32_t pixels) {
     const bool start = valid && (p.accumulate || train);
     if (start) {
         Pcg rng = b.rng[i];
-        int x = i % p.width, y = i / p.width;
-        float u = (x + rng.uniform()) / float(p.width);
-        float v = (y + rng.uniform()) / float(p.height);
-        pt_ray r;
-        camera_ray(p.camera, u, v, rng, r);
-        b.rng[i] = rng;
         CachePath s;
-        s.ox = r.origin.x; s.oy = r.origin.y; s.oz = r.origin.z; s.time = r.time;
-        s.dx = r.direction.x; s.dy = r.direction.y; s.dz = r.direction.z; s.bounce_pdf = 0;
-        s.tr = 1; s.tg = 1; s.tb = 1; s.prev_pdf = 0;
-        s.rr = 0; s.rg = 0; s.rb = 0; s.spread = 0;
-        s.ur = 1; s.ug = 1; s.ub = 1; s.a0 = 0;
-        s.sr = 0; s.sg = 0; s.sb = 0; s.depth = 0;
-        s.train = train ? slot : -1; s.vertices = -1; s.qdepth = 0; s.pad = 0;
+        camera_sample(p, i, rng, train ? slot : -1, p.spf, s);   // a training pixel trains on its first sample
+        b.rng[i] = rng;
         b.paths[i] = s;
+        if (p.accumulate) b.pixel_query_count[i] = 0;
     }
     push(start, i, b.queue[0], &b.counters[0]);
+}
+
+// A prediction of L / albedo, bounded by the brightest emitter: with no emitted radiance above
+// Le_max, no outgoing radiance exceeds albedo * Le_max (a diffuse, mirror or glass vertex
+// passes on at most albedo times its brightest incoming radiance).  A prediction outside
+// [0, Le_max] cannot be right; the clamp keeps a badly extrapolated query from becoming a
+// firefly.
+__device__ inline float bounded(float prediction, float bound) {
+    return prediction >= 0.0f ? fminf(prediction, bound) : 0.0f;
 }
 
 __device__ inline pt_ray cache_ray(const CachePath &s) {
@@ -323,13 +345,23 @@ __device__ inline void shade(const DeviceScene &scene, const Params &p, const Bu
     o.live = !o.finished;
 }
 
-// Book-keeping of a path that ended this bounce: its cache query (index `q`), or its radiance
-// into the pixel sum; a training path's end record.
-__device__ inline void retire(const Params &p, const Buffers &b, int32_t i, const CachePath &s, const ShadeOut &o, int32_t q) {
-    if (o.query) { b.queries[q] = o.q; b.aux[q] = o.aux; }
-    else if (p.accumulate) {
+// Book-keeping of a path sample that ended this bounce: its radiance into the pixel sum, its
+// cache query (index `q`) into the pixel's query list (the resolve step adds the weighted
+// prediction), a training path's end record.  Then the pixel's next sample starts, if any;
+// returns whether the path goes on.
+__device__ inline bool retire(const Params &p, const Buffers &b, int32_t i, CachePath &s, Pcg &rng, const ShadeOut &o, int32_t q) {
+    if (p.accumulate) {
         float *sum = b.sums + 3 * size_t(i);
         sum[0] += s.rr; sum[1] += s.rg; sum[2] += s.rb;
+    }
+    if (o.query) {
+        b.queries[q] = o.q;
+        b.aux[q] = o.aux;
+        if (p.accumulate) {
+            int32_t j = b.pixel_query_count[i];
+            b.pixel_queries[size_t(i) * p.spf + j] = q;
+            b.pixel_query_count[i] = j + 1;
+        }
     }
     if (s.train >= 0) {
         TrainEnd e;
@@ -338,6 +370,11 @@ __device__ inline void retire(const Params &p, const Buffers &b, int32_t i, cons
         e.vertices = s.vertices > 0 ? s.vertices : 0;
         b.ends[s.train] = e;
     }
+    if (s.samples_left > 1) {
+        camera_sample(p, i, rng, -1, s.samples_left - 1, s);
+        return true;
+    }
+    return false;
 }
 
 __global__ void shade_kernel(DeviceScene scene, Params p, Buffers b, int parity) {
@@ -351,19 +388,23 @@ __global__ void shade_kernel(DeviceScene scene, Params p, Buffers b, int parity)
         const int32_t i = valid ? in[k] : 0;
         ShadeOut o;
         CachePath s;
+        Pcg rng;
         if (valid) {
             s = b.paths[i];
             PathHit h = b.hits[i];
-            Pcg rng = b.rng[i];
+            rng = b.rng[i];
             shade(scene, p, b, i, s, h, rng, o);
-            b.rng[i] = rng;
-            b.paths[i] = s;
             if (o.shadow) b.shadows[i] = o.sr;
         }
-        push(o.live, i, out, &b.counters[parity ^ 1]);
-        push(o.shadow, i, b.shadow_queue, &b.counters[2]);
         const int32_t q = append(o.query, &b.counters[3]);
-        if (valid && o.finished) retire(p, b, i, s, o, q);
+        bool live = o.live;
+        if (valid) {
+            if (o.finished) live = retire(p, b, i, s, rng, o, q);
+            b.rng[i] = rng;
+            b.paths[i] = s;
+        }
+        push(live, i, out, &b.counters[parity ^ 1]);
+        push(o.shadow, i, b.shadow_queue, &b.counters[2]);
     }
 }
 
@@ -410,8 +451,7 @@ __global__ void finish_kernel(DeviceScene scene, Params p, Buffers b, int parity
             }
             if (o.finished) {
                 const int32_t q = o.query ? atomicAdd(&b.counters[3], 1) : -1;
-                retire(p, b, i, s, o, q);
-                break;
+                if (!retire(p, b, i, s, rng, o, q)) break;
             }
         }
         b.paths[i] = s;
@@ -445,18 +485,23 @@ __global__ void shadow_kernel(DeviceScene scene, Params p, Buffers b, int min_ac
     else persistent_walk<true>(scene, size_t(n), &b.fetch[1], min_active, kTieLastLeaf, get, done);
 }
 
-// Pixel sums of the paths that ended at a cache query.
-__global__ void resolve_kernel(Params p, Buffers b, int32_t capacity) {
-    const int32_t n = min(b.counters[3], capacity);
-    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&b.totals[1], (unsigned long long)n);
+// Pixel sums += weight x prediction of the pixel's queries, in sample order.
+__global__ void resolve_kernel(Params p, Buffers b, int32_t pixels) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&b.totals[1], (unsigned long long)b.counters[3]);
     if (!p.accumulate) return;
-    for (int32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const QueryAux a = b.aux[k];
-        const CachePath &s = b.paths[a.path];
-        float *sum = b.sums + 3 * size_t(a.path);
-        sum[0] += s.rr + a.wr * b.pred[3 * size_t(k)];
-        sum[1] += s.rg + a.wg * b.pred[3 * size_t(k) + 1];
-        sum[2] += s.rb + a.wb * b.pred[3 * size_t(k) + 2];
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < pixels; i += gridDim.x * blockDim.x) {
+        const int32_t n = b.pixel_query_count[i];
+        if (!n) continue;
+        float *sum = b.sums + 3 * size_t(i);
+        float acc[3] = {sum[0], sum[1], sum[2]};
+        for (int32_t j = 0; j < n; j++) {
+            const int32_t q = b.pixel_queries[size_t(i) * p.spf + j];
+            const QueryAux a = b.aux[q];
+            acc[0] += a.wr * bounded(b.pred[3 * size_t(q)], p.radiance_max[0]);
+            acc[1] += a.wg * bounded(b.pred[3 * size_t(q) + 1], p.radiance_max[1]);
+            acc[2] += a.wb * bounded(b.pred[3 * size_t(q) + 2], p.radiance_max[2]);
+        }
+        sum[0] = acc[0]; sum[1] = acc[1]; sum[2] = acc[2];
     }
 }
 
@@ -467,9 +512,9 @@ __global__ void targets_kernel(Params p, Buffers b) {
         const TrainEnd e = b.ends[t];
         float total[3] = {e.sr, e.sg, e.sb};
         if (e.query >= 0) {
-            total[0] += e.wr * b.pred[3 * size_t(e.query)];
-            total[1] += e.wg * b.pred[3 * size_t(e.query) + 1];
-            total[2] += e.wb * b.pred[3 * size_t(e.query) + 2];
+            total[0] += e.wr * bounded(b.pred[3 * size_t(e.query)], p.radiance_max[0]);
+            total[1] += e.wg * bounded(b.pred[3 * size_t(e.query) + 1], p.radiance_max[1]);
+            total[2] += e.wb * bounded(b.pred[3 * size_t(e.query) + 2], p.radiance_max[2]);
         }
         const int bucket = t % p.steps;
         for (int v = 0; v < e.vertices && v < kMaxSuffix; v++) {
@@ -518,13 +563,14 @@ struct pt_cached_renderer {
     int block = 256;
     int grid_extend = 0, grid_shade = 0, grid_shadow = 0, grid_finish = 0, grid_small = 0;
     DeviceBuffer paths, hits, shadows, queue0, queue1, shadow_queue, counters, fetch, totals, error, sums, rng, frame;
-    DeviceBuffer queries, aux, pred, vertices, ends, samples, targets;
+    DeviceBuffer queries, aux, pred, pixel_queries, pixel_query_count, vertices, ends, samples, targets;
     Buffers buf{};
     cudaStream_t stream = nullptr;
     Event start, stop;
-    cudaGraphExec_t exec[2] = {nullptr, nullptr};
+    bool training = true;               // online training on (pt_cached_training)
+    cudaGraphExec_t exec[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};   // [accumulate][training]
     ~pt_cached_renderer() {
-        for (auto &e : exec) if (e) cudaGraphExecDestroy(e);
+        for (auto &row : exec) for (auto &e : row) if (e) cudaGraphExecDestroy(e);
         if (cache) pt_cache_destroy(cache);
         if (stream) cudaStreamDestroy(stream);
     }
@@ -532,6 +578,8 @@ struct pt_cached_renderer {
     void record(int accumulate) {
         Params p = params;
         p.accumulate = accumulate;
+        if (!accumulate) p.spf = 1;                 // training-only frames: the training sample alone
+        if (!training) p.train_threshold = 0;   // no training paths: every pixel may end at the cache
         const DeviceScene &scene_view = scene->view;
         cudaStream_t st = stream;
         PT_CUDA(cudaMemsetAsync(buf.counters, 0, (5 + kMaxSteps) * sizeof(int32_t), st));
@@ -539,8 +587,10 @@ struct pt_cached_renderer {
         start_kernel<<<(pixels + 255) / 256, 256, 0, st>>>(p, buf, pixels);
         PT_CUDA(cudaGetLastError());
         // a few wavefront iterations carry the bulk of the paths; the fused kernel ends the rest
+        // (a pixel's samples run one after another: at most spf * (max_depth + 1) bounces)
         int parity = 0;
-        const int iterations = std::min(p.wavefront, p.max_depth + 1);
+        const int64_t bounces = int64_t(p.spf) * (p.max_depth + 1);
+        const int iterations = int(std::min<int64_t>(p.wavefront, bounces));
         for (int it = 0; it < iterations; it++) {
             extend_kernel<<<grid_extend, block, stack_bytes(block), st>>>(scene_view, p, buf, parity, g_query_config.min_active);
             shade_kernel<<<grid_shade, block, 0, st>>>(scene_view, p, buf, parity);
@@ -548,12 +598,12 @@ struct pt_cached_renderer {
             PT_CUDA(cudaGetLastError());
             parity ^= 1;
         }
-        if (iterations < p.max_depth + 1) {
+        if (iterations < bounces) {
             finish_kernel<<<grid_finish, block, 0, st>>>(scene_view, p, buf, parity);
             PT_CUDA(cudaGetLastError());
         }
         if (p.use_cache) {
-            cache_forward(cache, buf.queries, size_t(pixels), &buf.counters[3], buf.pred, st);
+            cache_forward(cache, buf.queries, query_capacity(), &buf.counters[3], buf.pred, st);
             resolve_kernel<<<grid_small, 256, 0, st>>>(p, buf, pixels);
             PT_CUDA(cudaGetLastError());
             if (p.train_threshold) {
@@ -568,24 +618,26 @@ struct pt_cached_renderer {
         frame_end_kernel<<<1, 32, 0, st>>>(p, buf);
         PT_CUDA(cudaGetLastError());
     }
+    size_t query_capacity() const { return size_t(pixels) * size_t(params.spf); }
     cudaGraphExec_t graph(int accumulate) {
-        if (exec[accumulate]) return exec[accumulate];
+        cudaGraphExec_t &slot = exec[accumulate][training ? 1 : 0];
+        if (slot) return slot;
         cudaGraph_t g = nullptr;
         PT_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
         try { record(accumulate); } catch (...) { cudaStreamEndCapture(stream, &g); if (g) cudaGraphDestroy(g); throw; }
         PT_CUDA(cudaStreamEndCapture(stream, &g));
-        cudaError_t e = cudaGraphInstantiate(&exec[accumulate], g, 0);
+        cudaError_t e = cudaGraphInstantiate(&slot, g, 0);
         cudaGraphDestroy(g);
         PT_CUDA(e);
-        return exec[accumulate];
+        return slot;
     }
 };
 
 namespace {
 void defaults(pt_cached_params &c) {
-    c.training_paths = 65536; c.train_steps = 4; c.suffix_bounces = 4; c.use_cache = 1; c.train = 1; c.use_graph = 1;
-    c.spread_threshold = 0.01f; c.learning_rate = 1e-2f; c.network_seed = 7; c.wavefront_iterations = 3;
-    c.query_specular = 0; c.weight_average = 0.99f; c.reserved = 0;
+    c.training_paths = 65536; c.train_steps = 1; c.suffix_bounces = 4; c.use_cache = 1; c.train = 1; c.use_graph = 1;
+    c.spread_threshold = 0.3f; c.learning_rate = 1e-2f; c.network_seed = 7; c.wavefront_iterations = 10;
+    c.query_specular = 1; c.weight_average = 0.99f; c.samples_per_frame = 4;
 }
 } // namespace
 
@@ -610,7 +662,8 @@ pt_status pt_cached_create(const pt_scene *scene, const pt_camera *camera, int w
         if (max_depth < 0 || max_depth > 1000) throw Error(PT_INVALID_ARGUMENT, "invalid bounce limit");
         if (cfg.training_paths < 0 || cfg.train_steps < 1 || cfg.train_steps > kMaxSteps || cfg.suffix_bounces < 1 ||
             cfg.suffix_bounces > kMaxSuffix || !(cfg.spread_threshold >= 0) || !(cfg.learning_rate > 0) ||
-            cfg.wavefront_iterations < 0 || !(cfg.weight_average >= 0 && cfg.weight_average < 1))
+            cfg.wavefront_iterations < 0 || !(cfg.weight_average >= 0 && cfg.weight_average < 1) ||
+            cfg.samples_per_frame < 1 || cfg.samples_per_frame > 64)
             throw Error(PT_INVALID_ARGUMENT, "invalid radiance-cache settings");
         for (const pt_vec3 &v : {camera->origin, camera->lower_left_corner, camera->horizontal, camera->vertical})
             if (!std::isfinite(v.x) || !std::isfinite(v.y) || !std::isfinite(v.z))
@@ -642,6 +695,7 @@ pt_status pt_cached_create(const pt_scene *scene, const pt_camera *camera, int w
             p.suffix_bounces = cfg.suffix_bounces;
             p.wavefront = cfg.wavefront_iterations;
             p.query_specular = cfg.query_specular ? 1 : 0;
+            p.spf = cfg.samples_per_frame;
             p.steps = cfg.train_steps;
             p.spread_c = cfg.spread_threshold;
             p.seed = seed;
@@ -649,6 +703,21 @@ pt_status pt_cached_create(const pt_scene *scene, const pt_camera *camera, int w
             p.train_threshold = training ? uint32_t(std::min(4294967295.0, std::ceil(fraction * 4294967296.0))) : 0u;
             p.train_capacity = capacity;
             p.bucket_capacity = training ? (capacity + p.steps - 1) / p.steps * p.suffix_bounces : 0;
+            {
+                // brightest emitted radiance: constant colour, image texel (<= 1) or colour x texel
+                std::vector<pt_material> mats(scene->materials.bytes() / sizeof(pt_material));
+                std::vector<pt_texture> texs(scene->textures.bytes() / sizeof(pt_texture));
+                if (!mats.empty()) PT_CUDA(cudaMemcpy(mats.data(), scene->materials.get(), mats.size() * sizeof(pt_material), cudaMemcpyDeviceToHost));
+                if (!texs.empty()) PT_CUDA(cudaMemcpy(texs.data(), scene->textures.get(), texs.size() * sizeof(pt_texture), cudaMemcpyDeviceToHost));
+                float bound[3] = {0, 0, 0};
+                for (const pt_material &m : mats) {
+                    if (m.type != PT_LIGHT || m.texture_id < 0 || size_t(m.texture_id) >= texs.size()) continue;
+                    const pt_texture &t = texs[size_t(m.texture_id)];
+                    const float c[3] = {t.color.x, t.color.y, t.color.z};
+                    for (int a = 0; a < 3; a++) bound[a] = std::max(bound[a], t.type == PT_TEX_IMAGE ? 1.0f : std::fabs(c[a]));
+                }
+                for (int a = 0; a < 3; a++) p.radiance_max[a] = bound[a];
+            }
             r->paths.resize(n * sizeof(CachePath));
             r->hits.resize(n * sizeof(PathHit));
             r->shadows.resize(n * sizeof(CacheShadow));
@@ -662,10 +731,13 @@ pt_status pt_cached_create(const pt_scene *scene, const pt_camera *camera, int w
             r->sums.resize(n * 3 * sizeof(float));
             r->rng.resize(n * sizeof(Pcg));
             r->frame.resize(sizeof(uint32_t));
+            r->pixel_query_count.resize(n * sizeof(int32_t));
             if (cfg.use_cache) {
-                r->queries.resize(n * sizeof(pt_cache_query));
-                r->aux.resize(n * sizeof(QueryAux));
-                r->pred.resize(n * 3 * sizeof(float));
+                const size_t nq = n * size_t(cfg.samples_per_frame);   // at most one query per sample
+                r->queries.resize(nq * sizeof(pt_cache_query));
+                r->aux.resize(nq * sizeof(QueryAux));
+                r->pred.resize(nq * 3 * sizeof(float));
+                r->pixel_queries.resize(nq * sizeof(int32_t));
             }
             if (training) {
                 r->vertices.resize(size_t(capacity) * kMaxSuffix * sizeof(TrainVertex));
@@ -682,6 +754,7 @@ pt_status pt_cached_create(const pt_scene *scene, const pt_camera *camera, int w
             b.error = r->error.get<int32_t>(); b.sums = r->sums.get<float>(); b.rng = r->rng.get<Pcg>();
             b.frame = r->frame.get<uint32_t>();
             b.queries = r->queries.get<pt_cache_query>(); b.aux = r->aux.get<QueryAux>(); b.pred = r->pred.get<float>();
+            b.pixel_queries = r->pixel_queries.get<int32_t>(); b.pixel_query_count = r->pixel_query_count.get<int32_t>();
             b.vertices = r->vertices.get<TrainVertex>(); b.ends = r->ends.get<TrainEnd>();
             b.samples = r->samples.get<pt_cache_query>(); b.targets = r->targets.get<float>();
             PT_CUDA(cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking));
@@ -709,8 +782,10 @@ pt_status pt_cached_destroy(pt_cached_renderer *r) { delete r; return PT_OK; }
 pt_status pt_cached_frames(pt_cached_renderer *r, int frames, int accumulate) {
     return guard([&]() {
         if (!r || frames <= 0 || (accumulate != 0 && accumulate != 1)) throw Error(PT_INVALID_ARGUMENT, "invalid frame request");
-        if (accumulate && frames > INT32_MAX - r->frames) throw Error(PT_INVALID_ARGUMENT, "invalid accumulated frame count");
-        if (!accumulate && !r->params.train_threshold) throw Error(PT_INVALID_ARGUMENT, "training-only frames need online training");
+        if (accumulate && int64_t(frames) * r->params.spf > int64_t(INT32_MAX - r->frames))
+            throw Error(PT_INVALID_ARGUMENT, "invalid accumulated sample count");
+        if (!accumulate && !(r->params.train_threshold && r->training))
+            throw Error(PT_INVALID_ARGUMENT, "training-only frames need online training");
         cudaGraphExec_t g = r->cfg.use_graph ? r->graph(accumulate) : nullptr;
         PT_CUDA(cudaEventRecord(r->start.get(), r->stream));
         for (int f = 0; f < frames; f++) {
@@ -726,7 +801,14 @@ pt_status pt_cached_frames(pt_cached_renderer *r, int frames, int accumulate) {
         float ms = 0;
         PT_CUDA(cudaEventElapsedTime(&ms, r->start.get(), r->stop.get()));
         r->milliseconds += ms;
-        if (accumulate) r->frames += frames;
+        if (accumulate) r->frames += frames * r->params.spf;
+    });
+}
+
+pt_status pt_cached_training(pt_cached_renderer *r, int on) {
+    return guard([&]() {
+        if (!r || (on != 0 && on != 1)) throw Error(PT_INVALID_ARGUMENT, "invalid training switch");
+        r->training = on == 1;
     });
 }
 

@@ -161,6 +161,7 @@ def library() -> C.CDLL:
         "pt_cached_destroy": (I, [P]),
         "pt_cached_frames": (I, [P, C.c_int, C.c_int]),
         "pt_cached_clear": (I, [P]),
+        "pt_cached_training": (I, [P, C.c_int]),
         "pt_cached_get_sums": (I, [P, P, S]),
         "pt_cached_stats": (I, [P, P, P, P, P, P, P]),
         "pt_cached_cache": (I, [P, P]),
@@ -627,10 +628,12 @@ class RadianceCache:
     def query(self, queries, count: int, out, stream=0) -> None:
         check(library().pt_cache_query_device(self._h, _ptr(queries), count, _ptr(out), stream))
 
-    def train(self, queries, targets, count: int, stream=0) -> float:
+    def train(self, queries, targets, count: int, stream=0, wait: bool = True):
+        """One Adam step; returns the batch's mean loss (wait=False: asynchronous, returns None)."""
         loss = C.c_float()
-        check(library().pt_cache_train_device(self._h, _ptr(queries), _ptr(targets), count, C.byref(loss), stream))
-        return loss.value
+        check(library().pt_cache_train_device(self._h, _ptr(queries), _ptr(targets), count,
+                                              C.byref(loss) if wait else None, stream))
+        return loss.value if wait else None
 
     def gradients(self, queries, targets, count: int):
         g = np.zeros(CACHE_WEIGHTS, np.float32)
@@ -661,7 +664,7 @@ class CachedParams(C.Structure):
                 ("use_cache", C.c_int32), ("train", C.c_int32), ("use_graph", C.c_int32),
                 ("spread_threshold", C.c_float), ("learning_rate", C.c_float), ("network_seed", C.c_uint64),
                 ("wavefront_iterations", C.c_int32), ("query_specular", C.c_int32),
-                ("weight_average", C.c_float), ("reserved", C.c_int32)]
+                ("weight_average", C.c_float), ("samples_per_frame", C.c_int32)]
 
 
 class CachedRenderer:
@@ -705,6 +708,10 @@ class CachedRenderer:
 
     def clear(self) -> None:
         check(library().pt_cached_clear(self._h))
+
+    def training(self, on: bool) -> None:
+        """Switch online training off (the network is frozen) or back on."""
+        check(library().pt_cached_training(self._h, int(on)))
 
     def sums(self) -> np.ndarray:
         out = np.zeros((self.height, self.width, 3), np.float32)

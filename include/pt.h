@@ -290,18 +290,20 @@ pt_status pt_cache_average(pt_cache *cache, float decay);
  * reference; use_cache = 0 gives the plain path tracer through the same kernels. */
 typedef struct pt_cached_params {
     int32_t training_paths;     /* per frame (default 65536) */
-    int32_t train_steps;        /* Adam steps per frame (4); the training samples are split between them */
+    int32_t train_steps;        /* Adam steps per frame (1); the training samples are split between them */
     int32_t suffix_bounces;     /* bounces traced beyond the query by training paths (4, at most 8) */
     int32_t use_cache;          /* 1: end paths at the cache; 0: plain path tracing */
     int32_t train;              /* 1: online training; 0: the network stays as it is */
     int32_t use_graph;          /* 1: one graph launch per frame; 0: the same kernels launched one by one */
-    float spread_threshold;     /* c of the termination rule (0.01) */
+    float spread_threshold;     /* c of the termination rule (0.3) */
     float learning_rate;        /* Adam learning rate (1e-2; beta 0.9 / 0.99) */
     uint64_t network_seed;      /* weight initialisation */
-    int32_t wavefront_iterations; /* bounces run as wavefront kernels before the fused kernel ends the rest (3) */
-    int32_t query_specular;     /* 0: paths end at diffuse vertices only; 1: also at metal and glass vertices */
+    int32_t wavefront_iterations; /* bounces run as wavefront kernels before the fused kernel ends the rest (10;
+                                   * about 2 + 2 x samples_per_frame suits) */
+    int32_t query_specular;     /* 1 (default): paths may also end at metal and glass vertices;
+                                 * 0: at diffuse vertices only */
     float weight_average;       /* decay of the weight average queries use (0.99; 0: the live weights) */
-    int32_t reserved;
+    int32_t samples_per_frame;  /* samples per pixel in one frame (4; 1..64); the network trains once per frame */
 } pt_cached_params;
 typedef struct pt_cached_renderer pt_cached_renderer;
 /* params == NULL: the defaults above. */
@@ -309,13 +311,17 @@ pt_status pt_cached_defaults(pt_cached_params *params);
 pt_status pt_cached_create(const pt_scene *scene, const pt_camera *camera, int width, int height, uint64_t seed, int max_depth,
                            const pt_cached_params *params, pt_cached_renderer **out);
 pt_status pt_cached_destroy(pt_cached_renderer *renderer);
-/* `frames` frames; accumulate = 0: training-only frames (only the training paths are traced and
- * the image is left alone), 1: every pixel is rendered and added to the image sums. */
+/* `frames` frames; accumulate = 0: training-only frames (only the training paths are traced, one
+ * sample each, and the image is left alone), 1: every pixel is rendered with samples_per_frame
+ * samples and added to the image sums. */
 pt_status pt_cached_frames(pt_cached_renderer *renderer, int frames, int accumulate);
+/* on = 0: later frames leave the network as it is (and trace no training paths); 1: online
+ * training again (when the renderer was created with training). */
+pt_status pt_cached_training(pt_cached_renderer *renderer, int on);
 /* Clears the image sums and frame count (the network and the pixels' RNG streams go on). */
 pt_status pt_cached_clear(pt_cached_renderer *renderer);
 pt_status pt_cached_get_sums(const pt_cached_renderer *renderer, float *rgb, size_t floats);
-/* frames: accumulated frames; kernel_ms: device time of all frames; rays: closest-hit + shadow
+/* frames: accumulated samples per pixel; kernel_ms: device time of all frames; rays: closest-hit + shadow
  * queries; queries: cache queries; samples: training samples; loss: mean loss of the last step. */
 pt_status pt_cached_stats(pt_cached_renderer *renderer, int *frames, float *kernel_ms, uint64_t *rays, uint64_t *queries,
                           uint64_t *samples, float *loss);

@@ -42,13 +42,25 @@ def test_plain_mode_equals_plain_renderer(cornell):
     scene, camera = cornell
     plain = pt.CudaRenderer(scene, camera, 96, 64, seed=3, max_depth=8)
     plain.add_samples(16)
-    cached = pt.CachedRenderer(scene, camera, 96, 64, seed=3, max_depth=8, use_cache=0)
-    cached.frames(16)
+    cached = pt.CachedRenderer(scene, camera, 96, 64, seed=3, max_depth=8, use_cache=0, samples_per_frame=4)
+    cached.frames(4)
     a, b = cached.sums().astype(np.float64).reshape(-1), plain.sums().astype(np.float64).reshape(-1)
     np.testing.assert_allclose(a, b, rtol=1e-4, atol=1e-4)
     st = cached.stats()
     assert st["frames"] == 16 and st["queries"] == 0 and st["samples"] == 0
     assert abs(st["rays"] - plain.rays_traced()) <= 0.001 * plain.rays_traced()
+
+
+def test_samples_per_frame_are_frames_in_one_launch(cornell):
+    """A pixel's samples run one after the other inside a frame, consuming its PCG stream and
+    adding to its sum in the order separate frames would."""
+    scene, camera = cornell
+    one = pt.CachedRenderer(scene, camera, 96, 64, seed=9, max_depth=8, use_cache=0, samples_per_frame=1)
+    one.frames(8)
+    eight = pt.CachedRenderer(scene, camera, 96, 64, seed=9, max_depth=8, use_cache=0, samples_per_frame=8)
+    eight.frames(1)
+    assert one.sums().tobytes() == eight.sums().tobytes()
+    assert one.stats()["frames"] == eight.stats()["frames"] == 8
 
 
 def test_graph_and_launches_agree_with_frozen_network(cornell):
@@ -89,7 +101,7 @@ def test_trained_cache_gains_over_plain_and_untrained(cornell, reference):
     """Same frame count: the trained cache has lower relMSE than the plain path tracer and
     than the same renderer with its network left untrained."""
     scene, camera = cornell
-    frames = 64
+    frames = 16                                     # x 4 samples per frame
     plain = pt.CachedRenderer(scene, camera, 96, 64, seed=11, max_depth=8, use_cache=0)
     plain.frames(frames)
     untrained = pt.CachedRenderer(scene, camera, 96, 64, seed=11, max_depth=8, train=0)
@@ -98,7 +110,7 @@ def test_trained_cache_gains_over_plain_and_untrained(cornell, reference):
     trained.train(400)
     trained.frames(frames)
     e_plain, e_untrained, e_trained = (rel_mse(r.image(), reference) for r in (plain, untrained, trained))
-    print(f"relMSE at {frames} frames: plain {e_plain:.3e}, untrained cache {e_untrained:.3e}, trained cache {e_trained:.3e}")
+    print(f"relMSE at {4 * frames} samples: plain {e_plain:.3e}, untrained cache {e_untrained:.3e}, trained cache {e_trained:.3e}")
     assert e_trained < e_plain
     assert e_trained < 0.5 * e_untrained
 
@@ -107,7 +119,8 @@ def test_rejects_bad_settings(cornell):
     scene, camera = cornell
     for bad in (dict(train_steps=0), dict(train_steps=9), dict(suffix_bounces=0), dict(suffix_bounces=9),
                 dict(training_paths=-1), dict(learning_rate=0.0), dict(spread_threshold=-1.0),
-                dict(wavefront_iterations=-1)):
+                dict(wavefront_iterations=-1), dict(samples_per_frame=0), dict(samples_per_frame=65),
+                dict(weight_average=1.0)):
         with pytest.raises(ValueError):
             pt.CachedRenderer(scene, camera, 8, 8, **bad)
     with pytest.raises(ValueError):
