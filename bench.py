@@ -48,11 +48,12 @@ def parse():
     ap.add_argument("--log2-rays", type=int, default=LOG2_RAYS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", choices=["query", "batch48", "cache"], default="query",
+    ap.add_argument("--workload", choices=["query", "batch48", "cache", "mlp"], default="query",
                     help="query: the closest-hit benchmark (default); batch48: 48 render jobs in one launch; "
                          "cache: radiance-cache renderer vs plain, time to a relMSE at 1920x1080")
     ap.add_argument("--jobs", type=int, default=48)
-    ap.add_argument("--ref-spp", type=int, default=65536, help="cache workload: samples of the FP64 reference image")
+    ap.add_argument("--ref-spp", type=int, default=65536,
+                    help="cache workload: samples of the FP64 reference image (0: time cached frames only)")
     ap.add_argument("--max-spp", type=int, default=4096, help="cache workload: sample budget of each curve")
     return ap.parse_args()
 
@@ -247,6 +248,62 @@ def crossing(curve, target):
     return None
 
 
+def mlp_timings(net, n_query: int = 1 << 21, n_train: int = 1 << 16, reps: int = 20):
+    """CUDA-event times of the radiance-cache network alone: a forward pass over n_query
+    queries and one Adam step (forward + backward + reduce + update) over n_train samples,
+    on seeded synthetic queries in a 10-unit box."""
+    import torch
+    q = torch.zeros((n_query, 13), dtype=torch.float32, device="cuda")
+    g = torch.Generator(device="cuda").manual_seed(5)
+    q[:, 0:3] = torch.rand(n_query, 3, device="cuda", generator=g) * 10
+    q[:, 3:6] = torch.nn.functional.normalize(torch.randn(n_query, 3, device="cuda", generator=g), dim=1)
+    q[:, 6:9] = torch.nn.functional.normalize(torch.randn(n_query, 3, device="cuda", generator=g), dim=1)
+    q[:, 9:12] = 0.5
+    q[:, 12] = 1.0
+    out = torch.zeros(n_query * 3, device="cuda")
+    tgt = torch.rand(n_query * 3, device="cuda", generator=g)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+    fwd_ms = timed(lambda: net.query(q, n_query, out))
+    train_ms = timed(lambda: net.train(q, tgt, n_train, wait=False))
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    tpeak = float(peaks.get("bf16_tflops", 1590.0))
+    fwd_tf = 41344.0 * n_query / (fwd_ms / 1e3) / 1e12
+    train_tf = 3 * 41344.0 * n_train / (train_ms / 1e3) / 1e12
+    return {"forward_queries": n_query, "forward_ms": fwd_ms, "forward_tflops": fwd_tf, "train_samples": n_train,
+            "train_step_ms": train_ms, "train_tflops": train_tf, "flop_per_query": 41344,
+            "flop_per_training_sample": 3 * 41344, "peak_tflops": tpeak,
+            "peak_kind": "measured" if peaks else "fallback", "launches_per_rep": {"forward": 1, "train": 3}}
+
+
+def run_mlp(args):
+    """The radiance-cache network alone: forward over 2^21 queries, Adam steps over 2^16 samples."""
+    import torch
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    net = pt.RadianceCache((0, 0, 0), (10, 10, 10), seed=1)
+    clocks = Clocks(int(os.environ.get("LOCAL_RANK", "0")))
+    m = mlp_timings(net, reps=max(1, args.steps))
+    clock = clocks.stop()
+    line = {"metric": "TFLOP/s radiance-cache MLP forward", "value": m["forward_tflops"], "unit": "TFLOP/s", "n_gpus": 1,
+            "steps": max(1, args.steps), "warmup": 3, "ms_per_step": m["forward_ms"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "bf16", "data": "synthetic",
+            "config": {"workload": "MLP 64-64x5-3 forward over 2^21 queries; Adam step over 2^16 samples"},
+            "roofline": {"bound": "tensor", "achieved": m["forward_tflops"], "peak": m["peak_tflops"], "unit": "TFLOP/s",
+                         "frac": m["forward_tflops"] / m["peak_tflops"], "traffic": None, "peak_kind": m["peak_kind"]},
+            "mlp": m, "clocks": clock, "gpu_launches": 4 * (max(1, args.steps) + 3)}
+    print(json.dumps(line), flush=True)
+
+
 def run_cache(args):
     """Radiance cache vs plain path tracing on the procedural 1M-triangle scene at 1920x1080,
     depth 12, MIS: relMSE-vs-time curves against an FP64-accumulated plain reference, the time
@@ -261,6 +318,28 @@ def run_cache(args):
     scene, cam = pt.procedural_scene(W, H)
     dev = pt.Scene(scene)
     build_s = time.perf_counter() - t
+    if args.ref_spp <= 0:
+        # frames only (no reference image, no curves): per-frame cost of the cached renderer
+        cache = pt.CachedRenderer(dev, cam, W, H, 1, D)
+        cache.train(max(1, args.warmup))
+        cache.frames(max(1, args.warmup))
+        a = cache.stats()
+        clocks = Clocks(local)
+        cache.frames(max(1, args.steps))
+        clock = clocks.stop()
+        b = cache.stats()
+        spf = cache.params.samples_per_frame
+        ms = b["kernel_ms"] - a["kernel_ms"]
+        line = {"metric": "ms per cached frame at 1080p", "value": ms / max(1, args.steps), "unit": "ms", "n_gpus": 1,
+                "steps": max(1, args.steps), "warmup": max(1, args.warmup), "ms_per_step": ms / max(1, args.steps),
+                "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "bf16+f32", "data": "synthetic",
+                "config": {"workload": "radiance-cache frames, procedural 1M-triangle scene, 1920x1080, depth 12",
+                           "samples_per_frame": spf},
+                "mrays_per_s": (b["rays"] - a["rays"]) / ms / 1e3,
+                "queries_per_frame": (b["queries"] - a["queries"]) / max(1, args.steps),
+                "samples_per_frame_trained": (b["samples"] - a["samples"]) / max(1, args.steps), "clocks": clock}
+        print(json.dumps(line), flush=True)
+        return
     # reference: plain renders of 256 spp with independent seeds, accumulated in float64
     chunks = max(2, args.ref_spp // 256)
     acc = np.zeros(W * H * 3)
@@ -332,37 +411,8 @@ def run_cache(args):
     p_1e3, p_1e3_wall = pick(plain_curve, 1e-3)
     c_1024, c_1024_wall = pick(cache_curve, plain_1024[2])
     eq = min(cache_curve, key=lambda c: abs(c[1] - plain_1024[1]))
-    # the MLP kernels alone: forward over 2^21 queries, one training step over 2^16 samples
-    net = cache.cache()
-    nq = 1 << 21
-    q = torch.zeros((nq, 13), dtype=torch.float32, device="cuda")
-    g = torch.Generator(device="cuda").manual_seed(5)
-    q[:, 0:3] = torch.rand(nq, 3, device="cuda", generator=g) * 10
-    q[:, 3:6] = torch.nn.functional.normalize(torch.randn(nq, 3, device="cuda", generator=g), dim=1)
-    q[:, 6:9] = torch.nn.functional.normalize(torch.randn(nq, 3, device="cuda", generator=g), dim=1)
-    q[:, 9:12] = 0.5
-    q[:, 12] = 1.0
-    out = torch.zeros(nq * 3, device="cuda")
-    tgt = torch.rand(nq * 3, device="cuda", generator=g)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-
-    def timed(fn, reps=20):
-        for _ in range(3):
-            fn()
-        torch.cuda.synchronize()
-        e0.record()
-        for _ in range(reps):
-            fn()
-        e1.record()
-        torch.cuda.synchronize()
-        return e0.elapsed_time(e1) / reps
-    fwd_ms = timed(lambda: net.query(q, nq, out))
-    nt = 1 << 16
-    train_ms = timed(lambda: net.train(q, tgt, nt, wait=False))
-    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
-    tpeak = float(peaks.get("bf16_tflops", 1590.0))
-    fwd_tf = 41344.0 * nq / (fwd_ms / 1e3) / 1e12
-    train_tf = 3 * 41344.0 * nt / (train_ms / 1e3) / 1e12
+    mlp = mlp_timings(cache.cache())
+    tpeak, fwd_tf = mlp["peak_tflops"], mlp["forward_tflops"]
     # CPU baseline: the reference's host renderer's ray rate on a 960x540 render of the same view,
     # turned into the time the plain method's rays to relMSE 1e-3 would take on these cores
     cpu = None
@@ -397,14 +447,13 @@ def run_cache(args):
         "reference": {"spp": chunks * 256, "noise_relmse": noise, "seconds": ref_s},
         "cache_stats": st,
         "roofline": {"bound": "tensor", "kernel": "mlp forward", "achieved": fwd_tf, "peak": tpeak, "unit": "TFLOP/s",
-                     "frac": fwd_tf / tpeak, "traffic": None, "peak_kind": "measured" if peaks else "fallback"},
-        "mlp": {"forward_ms_2^21": fwd_ms, "forward_tflops": fwd_tf, "train_step_ms_2^16": train_ms, "train_tflops": train_tf,
-                "flop_per_query": 41344, "flop_per_training_sample": 3 * 41344},
+                     "frac": fwd_tf / tpeak, "traffic": None, "peak_kind": mlp["peak_kind"]},
+        "mlp": mlp,
         "clocks": clock, "scene_build_s": build_s,
-        # per frame: start, 3 per wavefront iteration, the fused tail, forward, resolve, targets,
-        # 3 per Adam step (gradients, reduce, update), frame end
-        "gpu_launches": int((st["frames"] // spf + 32) * (1 + 3 * cache.params.wavefront_iterations + 1 + 3 +
-                                                        3 * cache.params.train_steps + 1)),
+        # per frame: start, the wavefront loop (7 kernels per pair, pairs counted on the device
+        # are not read back; 8 pairs is the typical count at 4 samples per frame), the fused tail,
+        # forward, resolve, targets, 3 per Adam step (gradients, reduce, update), frame end
+        "gpu_launches": int((st["frames"] // spf + 32) * (1 + 7 * 8 + 1 + 3 + 3 * cache.params.train_steps + 1)),
         "e2e": {"value": c_1e3_wall, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": W * H * 12,
                 "api": "pt_cached_frames + pt_cached_get_sums (host wall clock)"},
         "cpu_baseline": cpu,
@@ -422,6 +471,9 @@ def main():
         return
     if args.workload == "cache":
         run_cache(args)
+        return
+    if args.workload == "mlp":
+        run_mlp(args)
         return
     import torch
     import torch.distributed as dist

@@ -8,9 +8,9 @@
 //   start   : camera ray of every pixel (training-only frames: of the training pixels only);
 //             about `training_paths` pixels, picked by a hash of (seed, frame, pixel), also
 //             get a training slot for their first sample;
-//   extend / shade / shadow, `wavefront_iterations` times, then one fused kernel (a thread per
-//             path) runs the remaining paths to their end (a pixel's samples end within
-//             samples_per_frame * (max_depth + 1) bounces):
+//   extend / shade / shadow, in pairs, while at least `tail_paths` paths are live (a device-
+//             side WHILE loop in the frame's graph), then one fused kernel (a thread per path)
+//             runs the short tail to its end:
 //             shade does the MIS step, tracks the path's area spread
 //               a0 = |x0 - x1|^2 / (4 pi cos1),  sqrt(a) += sqrt(|x_{i-1} - x_i|^2 / (pdf_{i-1} cos_i)),
 //             and at the first diffuse vertex (past the primary hit) where a > c * a0 it ends the
@@ -87,7 +87,7 @@ struct alignas(16) TrainEnd {
 struct Params {
     pt_camera camera;
     int width, height, max_depth, wide;
-    int use_cache, suffix_bounces, steps, accumulate, wavefront, query_specular;
+    int use_cache, suffix_bounces, steps, accumulate, query_specular;
     int spf;                            // samples per pixel in this frame
     float spread_c;
     uint32_t train_threshold;           // a pixel trains when its hash is below this
@@ -110,6 +110,7 @@ struct Buffers {
     float *sums;
     Pcg *rng;
     uint32_t *frame;
+    unsigned long long *pairs;          // wavefront iteration pairs run in this frame
     pt_cache_query *queries;
     QueryAux *aux;
     float *pred;
@@ -547,6 +548,17 @@ __global__ void frame_end_kernel(Params p, Buffers b) {
     b.frame[0] += 1;
 }
 
+// One thread: go on with the WHILE loop while at least tail_paths paths are live (the fused
+// kernel ends a shorter tail); past the iteration bound the frame stops with an error.
+__global__ void control_kernel(Buffers b, cudaGraphConditionalHandle handle, int32_t tail_paths, unsigned long long max_pairs) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const int32_t live = b.counters[0];
+    const unsigned long long pair = ++*b.pairs;
+    bool go = live > 0 && live >= tail_paths;
+    if (go && pair >= max_pairs) { *b.error = 2; go = false; }
+    cudaGraphSetConditional(handle, go ? 1u : 0u);
+}
+
 } // namespace nrc
 } // namespace ptb
 
@@ -565,43 +577,52 @@ struct pt_cached_renderer {
     DeviceBuffer paths, hits, shadows, queue0, queue1, shadow_queue, counters, fetch, totals, error, sums, rng, frame;
     DeviceBuffer queries, aux, pred, pixel_queries, pixel_query_count, vertices, ends, samples, targets;
     Buffers buf{};
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr, body_stream = nullptr;
     Event start, stop;
+    int32_t tail_paths = 0;             // live paths below which the fused kernel ends the frame
+    int32_t *live_host = nullptr;       // pinned: live count read back by the launched form
+    DeviceBuffer pairs;
     bool training = true;               // online training on (pt_cached_training)
     cudaGraphExec_t exec[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};   // [accumulate][training]
     ~pt_cached_renderer() {
         for (auto &row : exec) for (auto &e : row) if (e) cudaGraphExecDestroy(e);
         if (cache) pt_cache_destroy(cache);
+        if (live_host) cudaFreeHost(live_host);
+        if (body_stream) cudaStreamDestroy(body_stream);
         if (stream) cudaStreamDestroy(stream);
     }
     // the launches of one frame (also what a graph captures)
-    void record(int accumulate) {
+    Params frame_params(int accumulate) const {
         Params p = params;
         p.accumulate = accumulate;
         if (!accumulate) p.spf = 1;                 // training-only frames: the training sample alone
-        if (!training) p.train_threshold = 0;   // no training paths: every pixel may end at the cache
-        const DeviceScene &scene_view = scene->view;
-        cudaStream_t st = stream;
+        if (!training) p.train_threshold = 0;       // no training paths: every pixel may end at the cache
+        return p;
+    }
+    // A pixel's samples run one after another: at most spf * (max_depth + 1) bounces, so the
+    // wavefront ends within that many iterations (the pair loop's bound, with a margin).
+    unsigned long long max_pairs(const Params &p) const {
+        return (unsigned long long)p.spf * (unsigned long long)(p.max_depth + 1) / 2 + 2;
+    }
+    void prologue(const Params &p, cudaStream_t st) {
         PT_CUDA(cudaMemsetAsync(buf.counters, 0, (5 + kMaxSteps) * sizeof(int32_t), st));
         PT_CUDA(cudaMemsetAsync(buf.fetch, 0, 2 * sizeof(unsigned long long), st));
+        PT_CUDA(cudaMemsetAsync(buf.pairs, 0, sizeof(unsigned long long), st));
         start_kernel<<<(pixels + 255) / 256, 256, 0, st>>>(p, buf, pixels);
         PT_CUDA(cudaGetLastError());
-        // a few wavefront iterations carry the bulk of the paths; the fused kernel ends the rest
-        // (a pixel's samples run one after another: at most spf * (max_depth + 1) bounces)
-        int parity = 0;
-        const int64_t bounces = int64_t(p.spf) * (p.max_depth + 1);
-        const int iterations = int(std::min<int64_t>(p.wavefront, bounces));
-        for (int it = 0; it < iterations; it++) {
-            extend_kernel<<<grid_extend, block, stack_bytes(block), st>>>(scene_view, p, buf, parity, g_query_config.min_active);
-            shade_kernel<<<grid_shade, block, 0, st>>>(scene_view, p, buf, parity);
-            shadow_kernel<<<grid_shadow, block, stack_bytes(block), st>>>(scene_view, p, buf, g_query_config.min_active);
-            PT_CUDA(cudaGetLastError());
-            parity ^= 1;
+    }
+    void iteration_pair(const Params &p, cudaStream_t st) {
+        for (int parity = 0; parity < 2; parity++) {
+            extend_kernel<<<grid_extend, block, stack_bytes(block), st>>>(scene->view, p, buf, parity, g_query_config.min_active);
+            shade_kernel<<<grid_shade, block, 0, st>>>(scene->view, p, buf, parity);
+            shadow_kernel<<<grid_shadow, block, stack_bytes(block), st>>>(scene->view, p, buf, g_query_config.min_active);
         }
-        if (iterations < bounces) {
-            finish_kernel<<<grid_finish, block, 0, st>>>(scene_view, p, buf, parity);
-            PT_CUDA(cudaGetLastError());
-        }
+        PT_CUDA(cudaGetLastError());
+    }
+    // the fused kernel ends the paths left in queue 0, then the network's part of the frame
+    void epilogue(const Params &p, cudaStream_t st) {
+        finish_kernel<<<grid_finish, block, 0, st>>>(scene->view, p, buf, 0);
+        PT_CUDA(cudaGetLastError());
         if (p.use_cache) {
             cache_forward(cache, buf.queries, query_capacity(), &buf.counters[3], buf.pred, st);
             resolve_kernel<<<grid_small, 256, 0, st>>>(p, buf, pixels);
@@ -618,14 +639,65 @@ struct pt_cached_renderer {
         frame_end_kernel<<<1, 32, 0, st>>>(p, buf);
         PT_CUDA(cudaGetLastError());
     }
+    // One frame launched kernel by kernel: wavefront iteration pairs while at least tail_paths
+    // paths are live (the live count read back after each pair), then the epilogue.
+    void launch_frame(int accumulate) {
+        const Params p = frame_params(accumulate);
+        cudaStream_t st = stream;
+        prologue(p, st);
+        const unsigned long long bound = max_pairs(p);
+        for (unsigned long long pair = 0;; pair++) {
+            iteration_pair(p, st);
+            PT_CUDA(cudaMemcpyAsync(live_host, &buf.counters[0], sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+            PT_CUDA(cudaStreamSynchronize(st));
+            if (*live_host < tail_paths) break;
+            if (pair + 1 >= bound) throw Error(PT_TIMEOUT, "wavefront did not drain within its iteration bound");
+        }
+        epilogue(p, st);
+    }
+    // The same frame as one graph: prologue, a WHILE node whose body is an iteration pair and
+    // the control kernel (the device decides when the tail is short), epilogue.
+    void capture_frame(int accumulate, cudaGraph_t *out) {
+        const Params p = frame_params(accumulate);
+        PT_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        try {
+            prologue(p, stream);
+            cudaStreamCaptureStatus status;
+            cudaGraph_t g = nullptr;
+            const cudaGraphNode_t *deps = nullptr;
+            size_t ndeps = 0;
+            PT_CUDA(cudaStreamGetCaptureInfo(stream, &status, nullptr, &g, &deps, &ndeps));
+            cudaGraphConditionalHandle handle;
+            PT_CUDA(cudaGraphConditionalHandleCreate(&handle, g, 1, cudaGraphCondAssignDefault));
+            cudaGraphNodeParams cp{};
+            cp.type = cudaGraphNodeTypeConditional;
+            cp.conditional.handle = handle;
+            cp.conditional.type = cudaGraphCondTypeWhile;
+            cp.conditional.size = 1;
+            cudaGraphNode_t loop;
+            PT_CUDA(cudaGraphAddNode(&loop, g, deps, ndeps, &cp));
+            cudaGraph_t body = cp.conditional.phGraph_out[0];
+            PT_CUDA(cudaStreamBeginCaptureToGraph(body_stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+            iteration_pair(p, body_stream);
+            control_kernel<<<1, 32, 0, body_stream>>>(buf, handle, tail_paths, max_pairs(p));
+            PT_CUDA(cudaGetLastError());
+            PT_CUDA(cudaStreamEndCapture(body_stream, &body));
+            PT_CUDA(cudaStreamUpdateCaptureDependencies(stream, &loop, 1, cudaStreamSetCaptureDependencies));
+            epilogue(p, stream);
+        } catch (...) {
+            cudaGraph_t g = nullptr;
+            cudaStreamEndCapture(stream, &g);
+            if (g) cudaGraphDestroy(g);
+            throw;
+        }
+        PT_CUDA(cudaStreamEndCapture(stream, out));
+    }
     size_t query_capacity() const { return size_t(pixels) * size_t(params.spf); }
     cudaGraphExec_t graph(int accumulate) {
         cudaGraphExec_t &slot = exec[accumulate][training ? 1 : 0];
         if (slot) return slot;
         cudaGraph_t g = nullptr;
-        PT_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-        try { record(accumulate); } catch (...) { cudaStreamEndCapture(stream, &g); if (g) cudaGraphDestroy(g); throw; }
-        PT_CUDA(cudaStreamEndCapture(stream, &g));
+        capture_frame(accumulate, &g);
         cudaError_t e = cudaGraphInstantiate(&slot, g, 0);
         cudaGraphDestroy(g);
         PT_CUDA(e);
@@ -636,7 +708,7 @@ struct pt_cached_renderer {
 namespace {
 void defaults(pt_cached_params &c) {
     c.training_paths = 65536; c.train_steps = 1; c.suffix_bounces = 4; c.use_cache = 1; c.train = 1; c.use_graph = 1;
-    c.spread_threshold = 0.3f; c.learning_rate = 1e-2f; c.network_seed = 7; c.wavefront_iterations = 10;
+    c.spread_threshold = 0.3f; c.learning_rate = 1e-2f; c.network_seed = 7; c.tail_paths = 0;
     c.query_specular = 1; c.weight_average = 0.99f; c.samples_per_frame = 4;
 }
 } // namespace
@@ -662,7 +734,7 @@ pt_status pt_cached_create(const pt_scene *scene, const pt_camera *camera, int w
         if (max_depth < 0 || max_depth > 1000) throw Error(PT_INVALID_ARGUMENT, "invalid bounce limit");
         if (cfg.training_paths < 0 || cfg.train_steps < 1 || cfg.train_steps > kMaxSteps || cfg.suffix_bounces < 1 ||
             cfg.suffix_bounces > kMaxSuffix || !(cfg.spread_threshold >= 0) || !(cfg.learning_rate > 0) ||
-            cfg.wavefront_iterations < 0 || !(cfg.weight_average >= 0 && cfg.weight_average < 1) ||
+            cfg.tail_paths < 0 || !(cfg.weight_average >= 0 && cfg.weight_average < 1) ||
             cfg.samples_per_frame < 1 || cfg.samples_per_frame > 64)
             throw Error(PT_INVALID_ARGUMENT, "invalid radiance-cache settings");
         for (const pt_vec3 &v : {camera->origin, camera->lower_left_corner, camera->horizontal, camera->vertical})
@@ -693,7 +765,6 @@ pt_status pt_cached_create(const pt_scene *scene, const pt_camera *camera, int w
             p.wide = (g_query_config.wide && scene->view.nodes4) ? (g_query_config.speculative ? 2 : 1) : 0;
             p.use_cache = cfg.use_cache ? 1 : 0;
             p.suffix_bounces = cfg.suffix_bounces;
-            p.wavefront = cfg.wavefront_iterations;
             p.query_specular = cfg.query_specular ? 1 : 0;
             p.spf = cfg.samples_per_frame;
             p.steps = cfg.train_steps;
@@ -758,6 +829,11 @@ pt_status pt_cached_create(const pt_scene *scene, const pt_camera *camera, int w
             b.vertices = r->vertices.get<TrainVertex>(); b.ends = r->ends.get<TrainEnd>();
             b.samples = r->samples.get<pt_cache_query>(); b.targets = r->targets.get<float>();
             PT_CUDA(cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking));
+            PT_CUDA(cudaStreamCreateWithFlags(&r->body_stream, cudaStreamNonBlocking));
+            PT_CUDA(cudaMallocHost(&r->live_host, sizeof(int32_t)));
+            r->pairs.resize(sizeof(unsigned long long));
+            b.pairs = r->pairs.get<unsigned long long>();
+            r->tail_paths = cfg.tail_paths > 0 ? cfg.tail_paths : std::max<int32_t>(16384, int32_t(n / 32));
             r->grid_extend = occupancy_grid((const void *)extend_kernel, r->block, stack_bytes(r->block));
             r->grid_shade = occupancy_grid((const void *)shade_kernel, r->block, 0);
             r->grid_shadow = occupancy_grid((const void *)shadow_kernel, r->block, stack_bytes(r->block));
@@ -790,12 +866,13 @@ pt_status pt_cached_frames(pt_cached_renderer *r, int frames, int accumulate) {
         PT_CUDA(cudaEventRecord(r->start.get(), r->stream));
         for (int f = 0; f < frames; f++) {
             if (g) PT_CUDA(cudaGraphLaunch(g, r->stream));
-            else r->record(accumulate);
+            else r->launch_frame(accumulate);
         }
         PT_CUDA(cudaEventRecord(r->stop.get(), r->stream));
         PT_CUDA(cudaEventSynchronize(r->stop.get()));
         int32_t error = 0;
         PT_CUDA(cudaMemcpy(&error, r->buf.error, sizeof error, cudaMemcpyDeviceToHost));
+        if (error == 2) throw Error(PT_TIMEOUT, "wavefront did not drain within its iteration bound");
         if (error) throw Error(PT_STACK_OVERFLOW, "CUDA traversal stack overflow");
         cache_status(r->cache);
         float ms = 0;

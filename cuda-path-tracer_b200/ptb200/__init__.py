@@ -663,7 +663,7 @@ class CachedParams(C.Structure):
     _fields_ = [("training_paths", C.c_int32), ("train_steps", C.c_int32), ("suffix_bounces", C.c_int32),
                 ("use_cache", C.c_int32), ("train", C.c_int32), ("use_graph", C.c_int32),
                 ("spread_threshold", C.c_float), ("learning_rate", C.c_float), ("network_seed", C.c_uint64),
-                ("wavefront_iterations", C.c_int32), ("query_specular", C.c_int32),
+                ("tail_paths", C.c_int32), ("query_specular", C.c_int32),
                 ("weight_average", C.c_float), ("samples_per_frame", C.c_int32)]
 
 

@@ -298,8 +298,8 @@ typedef struct pt_cached_params {
     float spread_threshold;     /* c of the termination rule (0.3) */
     float learning_rate;        /* Adam learning rate (1e-2; beta 0.9 / 0.99) */
     uint64_t network_seed;      /* weight initialisation */
-    int32_t wavefront_iterations; /* bounces run as wavefront kernels before the fused kernel ends the rest (10;
-                                   * about 2 + 2 x samples_per_frame suits) */
+    int32_t tail_paths;         /* live paths below which one fused kernel ends the frame's tail
+                                 * (0: max(16384, pixels / 32)) */
     int32_t query_specular;     /* 1 (default): paths may also end at metal and glass vertices;
                                  * 0: at diffuse vertices only */
     float weight_average;       /* decay of the weight average queries use (0.99; 0: the live weights) */

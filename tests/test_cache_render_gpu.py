@@ -119,7 +119,7 @@ def test_rejects_bad_settings(cornell):
     scene, camera = cornell
     for bad in (dict(train_steps=0), dict(train_steps=9), dict(suffix_bounces=0), dict(suffix_bounces=9),
                 dict(training_paths=-1), dict(learning_rate=0.0), dict(spread_threshold=-1.0),
-                dict(wavefront_iterations=-1), dict(samples_per_frame=0), dict(samples_per_frame=65),
+                dict(tail_paths=-1), dict(samples_per_frame=0), dict(samples_per_frame=65),
                 dict(weight_average=1.0)):
         with pytest.raises(ValueError):
             pt.CachedRenderer(scene, camera, 8, 8, **bad)
