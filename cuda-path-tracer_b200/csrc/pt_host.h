@@ -57,3 +57,6 @@ void build_sah(FlatScene &scene, int threads);
 int hardware_threads();
 
 } // namespace ptb
+
+// The C ABI's host-owned flat scene handle (include/pt_workloads.h).
+struct pt_flat { ptb::FlatScene scene; };

@@ -8,7 +8,6 @@
 #include "pt_api_common.h"
 #include "../../include/pt_workloads.h"
 
-struct pt_flat { ptb::FlatScene scene; };
 
 namespace ptb {
 namespace {

@@ -4,6 +4,7 @@ Mirrors the reference renderer surface of AdmiralHeathCL/cuda-path-tracer:
 
 * ``cuda_device_available()``            — src/cuda/cuda_renderer.h:8
 * ``CudaRenderer``                        — class cuda_renderer, src/cuda/cuda_renderer.h:10-29
+* ``obj_scene``                           — load_obj + obj_scene, src/scene/obj_loader.h, obj_scene.h
 * ``cuda_query_rays(scene, rays, brute)`` — src/cuda/cuda_renderer.h:32
 * numpy record dtypes with the byte layout of the flat transfer records (src/flat/flat_data.h).
 
@@ -126,6 +127,7 @@ def library() -> C.CDLL:
         "pt_workload_cornell": (I, [I, I, P, P]),
         "pt_procedural_defaults": (None, [P]),
         "pt_workload_procedural": (I, [P, I, I, P, P]),
+        "pt_workload_obj": (I, [C.c_char_p, I, I, P, P, P, P, P, P, S]),
         "pt_rays_camera": (I, [P, I, I, U64, U64, S, P]),
         "pt_rays_surface": (I, [P, U64, U64, S, P, P, I]),
         "pt_rays_bounce": (I, [P, P, P, S, U64, U64, P, I]),
@@ -310,6 +312,22 @@ def procedural_scene(width: int = 960, height: int = 600, **overrides) -> tuple[
     check(lib.pt_workload_procedural(C.byref(p), width, height, C.byref(h), cam.ctypes.data))
     try:
         return _flat_from_handle(h), cam
+    finally:
+        lib.pt_flat_destroy(h)
+
+
+def obj_scene(path, width: int, height: int, scale=(1, 1, 1), rotate=(0, 0, 0), translate=(0, 0, 0)):
+    """OBJ/MTL import and the reference's preview stage (pt_workload_obj): (FlatScene, camera,
+    warnings) for a width x height render, as `ray_tracer --obj path` sets it up."""
+    lib = library()
+    h = C.c_void_p()
+    cam = np.zeros(1, CAMERA)
+    f = lambda v: (C.c_float * 3)(*[float(x) for x in v])
+    warn = C.create_string_buffer(4096)
+    check(lib.pt_workload_obj(str(path).encode(), width, height, f(scale), f(rotate), f(translate), C.byref(h),
+                              cam.ctypes.data, warn, 4096))
+    try:
+        return _flat_from_handle(h), cam, warn.value.decode()
     finally:
         lib.pt_flat_destroy(h)
 

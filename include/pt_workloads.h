@@ -57,6 +57,17 @@ void pt_procedural_defaults(pt_procedural_params *params);
 pt_status pt_workload_procedural(const pt_procedural_params *params, int width, int height,
                                  pt_flat **out, pt_camera *camera);
 
+/* The reference's OBJ import and preview stage (src/scene/obj_loader.h:116-237,
+ * src/scene/obj_scene.h:10-31; what `ray_tracer --obj FILE` renders): the OBJ's triangles with
+ * its MTL materials (Lambertian with Kd or a Kd-tinted PNG/PPM map_Kd, mirror for illum 3/5/8,
+ * glass for illum 4/6/7/9, emitter when Ke > 0), transformed by scale, then X/Y/Z rotation in
+ * degrees, then translation (any of the three may be NULL), a ground sphere (albedo 0.55) and an
+ * emitting sphere (radiance 3) sized to the mesh, and the 40-degree camera that frames it for a
+ * width x height image.  Binned-SAH BVH.  Warnings (simplified materials, skipped faces) go to
+ * `warnings` (may be NULL).  JPEG textures are rejected (PT_INVALID_ARGUMENT). */
+pt_status pt_workload_obj(const char *path, int width, int height, const float scale[3], const float rotate[3],
+                          const float translate[3], pt_flat **out, pt_camera *camera, char *warnings, size_t capacity);
+
 /* Camera rays of an image, one PCG stream per ray: ray k covers pixel k mod (w*h), jittered like
  * trace_pixel_sample (src/renderer/transport.h:232-239) with its stream seeded (seed, first+k). */
 pt_status pt_rays_camera(const pt_camera *camera, int width, int height, uint64_t seed, uint64_t first,
