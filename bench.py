@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--ref-spp", type=int, default=65536,
                     help="cache workload: samples of the FP64 reference image (0: time cached frames only)")
     ap.add_argument("--max-spp", type=int, default=4096, help="cache workload: sample budget of each curve")
+    ap.add_argument("--no-graph", action="store_true",
+                    help="cache frames: launch the kernels one by one instead of one graph per frame (for profilers)")
     return ap.parse_args()
 
 
@@ -320,7 +322,7 @@ def run_cache(args):
     build_s = time.perf_counter() - t
     if args.ref_spp <= 0:
         # frames only (no reference image, no curves): per-frame cost of the cached renderer
-        cache = pt.CachedRenderer(dev, cam, W, H, 1, D)
+        cache = pt.CachedRenderer(dev, cam, W, H, 1, D, use_graph=0 if args.no_graph else 1)
         cache.train(max(1, args.warmup))
         cache.frames(max(1, args.warmup))
         a = cache.stats()
@@ -334,7 +336,7 @@ def run_cache(args):
                 "steps": max(1, args.steps), "warmup": max(1, args.warmup), "ms_per_step": ms / max(1, args.steps),
                 "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "bf16+f32", "data": "synthetic",
                 "config": {"workload": "radiance-cache frames, procedural 1M-triangle scene, 1920x1080, depth 12",
-                           "samples_per_frame": spf},
+                           "samples_per_frame": spf, "graph": not args.no_graph},
                 "mrays_per_s": (b["rays"] - a["rays"]) / ms / 1e3,
                 "queries_per_frame": (b["queries"] - a["queries"]) / max(1, args.steps),
                 "samples_per_frame_trained": (b["samples"] - a["samples"]) / max(1, args.steps), "clocks": clock}
