@@ -1,12 +1,12 @@
-// pt_image.cpp — texture images for OBJ import: PNG (inflated with zlib) and PPM (P3, P6), turned
+// pt_image.cpp — texture images for OBJ import: PNG (inflated with zlib), PPM (P3, P6) and
+// baseline JPEG (pt_jpeg.cpp), turned
 // into 8-bit RGB rows top first, the form the reference's image_texture holds
 // (src/textures/texture.h:65-72 loads with 3 channels and indexes data[3*i + 3*nx*j]).
 //
 // PNG reduction to RGB follows what that loader (stb_image with 3 requested channels) does:
 // grey g -> (g, g, g), alpha dropped, palette entries looked up, 16-bit samples keep their high
 // byte, 1/2/4-bit grey scaled to 0..255 (x255, x85, x17).  Interlaced PNGs are de-interlaced
-// (Adam7).  JPEG is not decoded here: the reference's loader uses its own integer IDCT and
-// chroma upsampling, whose rounding this library does not reproduce.
+// (Adam7).  Baseline JPEG goes to pt_jpeg.cpp.
 #include <cctype>
 #include <cstdint>
 #include <cstdio>
@@ -205,7 +205,7 @@ bool load_image(const std::string &path, Image &img, std::string &err) {
     bool ok;
     if (file.size() >= 8 && file[0] == 137 && file[1] == 'P' && file[2] == 'N' && file[3] == 'G') ok = decode_png(file, img, err);
     else if (file.size() >= 3 && file[0] == 'P' && (file[1] == '6' || file[1] == '3')) ok = decode_ppm(file, img, err);
-    else if (file.size() >= 3 && file[0] == 0xFF && file[1] == 0xD8) { err = "JPEG textures are not supported (convert to PNG)"; ok = false; }
+    else if (file.size() >= 3 && file[0] == 0xFF && file[1] == 0xD8) ok = decode_jpeg(file, img, err);
     else { err = "unknown image format"; ok = false; }
     if (!ok) err = path + ": " + err;
     return ok;

@@ -13,5 +13,7 @@ struct Image {
 
 // false (and `err`) for a missing file, an unknown or unsupported format, or corrupt data.
 bool load_image(const std::string &path, Image &img, std::string &err);
+// Baseline JPEG (pt_jpeg.cpp).
+bool decode_jpeg(const std::vector<unsigned char> &file, Image &img, std::string &err);
 
 } // namespace ptb

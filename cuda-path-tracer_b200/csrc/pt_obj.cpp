@@ -571,7 +571,8 @@ extern "C" pt_status pt_workload_obj(const char *path, int width, int height, co
             if (!std::isfinite(radius)) throw Error(PT_INVALID_ARGUMENT, "OBJ bounds exceed camera range");
             const float aspect = float(width) / float(height);
             float half_angle = float(std::atan(std::tan(20 * M_PI / 180) * double(std::fmin(1.0f, aspect))));
-            float focus = float(double(1.2f * radius) / std::sin(double(half_angle)));
+            // the reference's sin(half_angle) takes the float overload (its tan and atan take doubles)
+            float focus = (1.2f * radius) / std::sin(half_angle);
             f3 lookfrom = lookat + focus * unit(mk(0.6f, 0.35f, 1.0f));
             int32_t floor_mat = add_material(s, PT_DIFFUSE, mk(0, 0, 0), 0, 1, add_texture(s, constant_record(mk(0.55f, 0.55f, 0.55f))));
             int32_t light_mat = add_material(s, PT_LIGHT, mk(0, 0, 0), 0, 1, add_texture(s, constant_record(mk(3, 3, 3))));

@@ -5,8 +5,9 @@ The fixtures are small files of this project's own making that exercise the impo
 triangles, quads split along either diagonal, a concave hexagon and a pentagon (ear clipping),
 1-based and negative indices, v/vt/vn, v//vn and bare v corners, a degenerate face, usemtl of
 every material kind (Lambertian, Kd-tinted texture with -s/-o/-clamp, mirror, glass, emitter,
-an unknown name), and PNG textures in several encodings (RGB, RGBA, grey+alpha, 16-bit grey,
-4-bit palette, Adam7-interlaced RGB, 1-bit grey).  The expected scenes come from the
+an unknown name), PNG textures in several encodings (RGB, RGBA, grey+alpha, 16-bit grey,
+4-bit palette, Adam7-interlaced RGB, 1-bit grey) and baseline JPEG textures (4:2:0 at an odd
+size, 4:2:2, 4:4:4, grey, restart intervals; written with Pillow).  The expected scenes come from the
 reference's obj_scene + flatten_scene compiled from its sources (oracle/_ref/libref_cpu.so):
 
     make -C oracle ref REF=/root/reference && python tests/golden/make_obj_golden.py
@@ -105,6 +106,17 @@ def write_fixtures():
     png(OBJ / "grey1.png", W, H, 0, 1, lambda y: np.packbits(bits[y]).tobytes())
     inter = g.integers(0, 256, (H, W, 3), dtype=np.uint8)
     png(OBJ / "interlaced.png", W, H, 2, 8, lambda y: [[inter[r, x].tobytes() for x in range(W)] for r in range(H)], interlace=True)
+    from PIL import Image
+    photo = np.zeros((29, 37, 3), np.uint8)
+    yy, xx = np.mgrid[0:29, 0:37]
+    photo[..., 0] = (128 + 100 * np.sin(xx / 3.0)).astype(np.uint8)
+    photo[..., 1] = (128 + 90 * np.cos(yy / 4.0 + xx / 7.0)).astype(np.uint8)
+    photo[..., 2] = g.integers(0, 256, (29, 37), dtype=np.uint8)
+    Image.fromarray(photo).save(OBJ / "jpeg420.jpg", quality=80, subsampling=2)
+    Image.fromarray(photo).save(OBJ / "jpeg422.jpg", quality=90, subsampling=1)
+    Image.fromarray(photo).save(OBJ / "jpeg444.jpg", quality=60, subsampling=0, restart_marker_blocks=3)
+    Image.fromarray(photo[..., 1]).save(OBJ / "jpeg_grey.jpg", quality=75)
+    Image.fromarray(photo[:24, :32]).save(OBJ / "jpeg_restart.jpg", quality=95, subsampling=2, restart_marker_rows=1)
     (OBJ / "fixture.mtl").write_text("""# materials of every kind the import maps
 newmtl plain
 Kd 0.8 0.3 0.1
@@ -132,6 +144,21 @@ map_Kd -clamp off grey1.png
 newmtl tex_inter
 Kd 0.6 0.6 0.6
 map_Kd interlaced.png
+newmtl jpg420
+Kd 1 1 1
+map_Kd jpeg420.jpg
+newmtl jpg422
+Kd 0.9 0.9 0.9
+map_Kd jpeg422.jpg
+newmtl jpg444
+Kd 1 0.8 0.6
+map_Kd jpeg444.jpg
+newmtl jpggrey
+Kd 1 1 1
+map_Kd jpeg_grey.jpg
+newmtl jpgrst
+Kd 1 1 1
+map_Kd -clamp on jpeg_restart.jpg
 newmtl mirror
 Ks 0.8 0.7 0.6
 illum 5
@@ -160,7 +187,8 @@ Ns 20
         n = g.normal(size=3)
         nrms.append(n)
         lines.append("vn %.6f %.6f %.6e" % tuple(n))
-    mats = ["plain", "clamped", "tex_rgb", "tex_rgba", "tex_ga", "tex_16", "tex_pal", "tex_bits", "tex_inter", "mirror",
+    mats = ["plain", "clamped", "tex_rgb", "tex_rgba", "tex_ga", "tex_16", "tex_pal", "tex_bits", "tex_inter",
+            "jpg420", "jpg422", "jpg444", "jpggrey", "jpgrst", "mirror",
             "glass", "lamp", "faded", "missing_name", None]
     for k, mat in enumerate(mats):
         if mat is not None:

@@ -9,6 +9,8 @@ bitwise, and the camera bitwise.
 """
 from __future__ import annotations
 
+import hashlib
+from functools import lru_cache
 from pathlib import Path
 
 import numpy as np
@@ -30,7 +32,7 @@ def texture_key(textures, pixels, tid):
     if t["type"] == pt.TEX_IMAGE:
         n = int(t["width"]) * int(t["height"]) * 3
         off = int(t["byte_offset"])
-        return ("image", int(t["width"]), int(t["height"]), pixels[off:off + n].tobytes())
+        return ("image", int(t["width"]), int(t["height"]), hashlib.sha256(pixels[off:off + n].tobytes()).hexdigest())
     return ("map", t["color"].tobytes(), t["scale"].tobytes(), t["offset"].tobytes(), int(t["clamp"]),
             texture_key(textures, pixels, int(t["image_id"])))
 
@@ -47,11 +49,12 @@ def material_key(scene, mid):
 
 def triangle_keys(scene):
     keys = []
+    mat = lru_cache(maxsize=None)(lambda mid: material_key(scene, mid))
     for t in scene.triangles:
         smooth = int(t["smooth"])
         normals = b"".join(t[f].tobytes() for f in ("n0", "n1", "n2")) if smooth else b""
         keys.append((b"".join(t[f].tobytes() for f in ("v0", "v1", "v2")), smooth, normals,
-                     b"".join(t[f].tobytes() for f in ("uv0", "uv1", "uv2")), material_key(scene, int(t["material_id"]))))
+                     b"".join(t[f].tobytes() for f in ("uv0", "uv1", "uv2")), mat(int(t["material_id"]))))
     return sorted(keys, key=repr)
 
 
@@ -106,7 +109,11 @@ def test_obj_import_errors(tmp_path):
     (tmp_path / "j.mtl").write_text("newmtl j\nmap_Kd t.jpg\n")
     (tmp_path / "t.jpg").write_bytes(b"\xff\xd8\xff\xe0" + bytes(16))
     jpg.write_text("mtllib j.mtl\nusemtl j\nv 0 0 0\nv 1 0 0\nv 0 1 0\nf 1 2 3\n")
-    with pytest.raises(ValueError, match="JPEG"):
+    with pytest.raises(ValueError, match="JPEG: bad marker length"):
+        pt.obj_scene(jpg, 10, 10)
+    from PIL import Image
+    Image.fromarray(np.full((16, 16, 3), 90, np.uint8)).save(tmp_path / "t.jpg", progressive=True)
+    with pytest.raises(ValueError, match="progressive"):
         pt.obj_scene(jpg, 10, 10)
     tri = tmp_path / "t.obj"
     tri.write_text("v 0 0 0\nv 1 0 0\nv 0 1 0\nf 1 2 3\n")
