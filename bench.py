@@ -48,7 +48,7 @@ def parse():
     ap.add_argument("--log2-rays", type=int, default=LOG2_RAYS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", choices=["query", "batch48", "cache", "mlp"], default="query",
+    ap.add_argument("--workload", choices=["query", "batch48", "cache", "mlp", "render"], default="query",
                     help="query: the closest-hit benchmark (default); batch48: 48 render jobs in one launch; "
                          "cache: radiance-cache renderer vs plain, time to a relMSE at 1920x1080")
     ap.add_argument("--jobs", type=int, default=48)
@@ -463,6 +463,80 @@ def run_cache(args):
     print(json.dumps(line), flush=True)
 
 
+def run_render(args):
+    """The progressive renderer on the procedural 1M-triangle scene, 960x600, 64 spp, bounce limit
+    8, MIS (one step = a full 64-spp render from a reset), beside the reference's own CUDA
+    renderer built with its bounce limit set to 8 ("patched reference", oracle/_ref) on the same
+    GPU: Mrays/s = rays traced / kernel time, as the reference reports it, and the two images
+    compared bitwise."""
+    import torch
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    W, H, SPP, D = 960, 600, 64, 8
+    t = time.perf_counter()
+    scene, cam = pt.procedural_scene(W, H)
+    dev = pt.Scene(scene)
+    build_s = time.perf_counter() - t
+    r = pt.CudaRenderer(dev, cam, W, H, 1, max_depth=D)
+    for _ in range(max(1, args.warmup)):
+        r.reset(cam)
+        r.add_samples(SPP)
+    clocks = Clocks(local)
+    ms = rays = 0.0
+    wall = 0.0
+    steps = max(1, args.steps)
+    img = None
+    for _ in range(steps):
+        r.reset(cam)
+        t = time.perf_counter()
+        r.add_samples(SPP)
+        img = r.image()
+        wall += time.perf_counter() - t
+        ms += r.kernel_milliseconds()
+        rays += r.rays_traced()
+    clock = clocks.stop()
+    value = rays / ms / 1e3
+    ref_line = None
+    sys.path.insert(0, str(ROOT / "oracle"))
+    from oracle_bind import RefGpu, ref_gpu_so, RefCpu, REF_CPU_SO
+    if ref_gpu_so(D).exists():
+        gpu = RefGpu(D)
+        rr = gpu.renderer(scene, cam, W, H, 1, mis=True)
+        rr.add_samples(SPP)                    # warm-up render
+        rr.close()
+        rms = rrays = 0.0
+        for _ in range(steps):
+            rr = gpu.renderer(scene, cam, W, H, 1, mis=True)
+            rr.add_samples(SPP)
+            _, kms, kr = rr.stats()
+            rms += kms
+            rrays += kr
+            same = rr.image().tobytes() == img.tobytes()
+            rr.close()
+        ref_line = {"mrays_per_s": rrays / rms / 1e3, "ms_per_render": rms / steps,
+                    "kind": "reference cuda_renderer, bounce limit 8 (patched reference), same GPU",
+                    "images_bit_identical": bool(same), "speedup": value / (rrays / rms / 1e3)}
+    cpu = None
+    if REF_CPU_SO.exists():
+        small, small_cam = pt.procedural_scene(240, 150)
+        threads = os.cpu_count() or 1
+        t = time.perf_counter()
+        _, _, crays = RefCpu().render(small, small_cam, 240, 150, 1, [4], nthreads=threads)
+        dt = time.perf_counter() - t
+        cpu = {"value": crays / dt / 1e6, "unit": "Mrays/s", "cores": threads, "kind": "reference",
+               "sample": f"reference trace_pixel_sample (bounce limit 50) on 240x150 x 4 spp: {crays} rays in {dt:.2f} s"}
+    line = {"metric": "Mrays/s render (procedural 1M, 960x600, 64 spp, depth 8, MIS)", "value": value, "unit": "Mrays/s",
+            "n_gpus": 1, "steps": steps, "warmup": max(1, args.warmup), "ms_per_step": ms / steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "progressive render of the procedural 1M-triangle scene, 960x600, 64 spp, bounce limit 8, MIS",
+                       "l2": "frame state > L2"},
+            "rays_per_render": rays / steps, "reference_gpu": ref_line, "clocks": clock, "scene_build_s": build_s,
+            "e2e": {"value": rays / wall / 1e6, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": W * H * 12,
+                    "api": "pt_add_samples + pt_get_image (host wall clock)"},
+            "cpu_baseline": cpu}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -476,6 +550,9 @@ def main():
         return
     if args.workload == "mlp":
         run_mlp(args)
+        return
+    if args.workload == "render":
+        run_render(args)
         return
     import torch
     import torch.distributed as dist

@@ -281,13 +281,21 @@ class RefCpu:
             self.lib.ref_mesh_free(h)
 
 
-class RefGpu:
-    """The reference's own CUDA renderer and cuda_query_rays (sm_100a build)."""
+def ref_gpu_so(depth=None) -> Path:
+    """oracle/_ref/libref_cuda.so, or the patched build whose bounce limit is `depth` (8 or 12)."""
+    return REF_GPU_SO if depth is None else REF_GPU_SO.with_name(f"libref_cuda_d{depth}.so")
 
-    def __init__(self):
-        if not REF_GPU_SO.exists():
-            raise RuntimeError("oracle/_ref/libref_cuda.so is not built (make -C oracle ref)")
-        lib = C.CDLL(str(REF_GPU_SO))
+
+class RefGpu:
+    """The reference's own CUDA renderer and cuda_query_rays (sm_100a build).  depth=8 or 12
+    loads the "patched reference": the same sources with trace_color's bounce limit of 50
+    (src/renderer/transport.h:174,193) set to that depth (oracle/Makefile)."""
+
+    def __init__(self, depth=None):
+        so = ref_gpu_so(depth)
+        if not so.exists():
+            raise RuntimeError(f"{so} is not built (make -C oracle ref)")
+        lib = C.CDLL(str(so))
         sig = {
             "refgpu_last_error": (C.c_char_p, []),
             "refgpu_available": (I, [C.c_char_p, S]),

@@ -21,7 +21,7 @@ import numpy as np
 import pytest
 
 import ptb200 as pt
-from oracle_bind import Oracle, RefGpu, REF_GPU_SO
+from oracle_bind import Oracle, RefGpu, REF_GPU_SO, ref_gpu_so
 
 pytestmark = pytest.mark.gpu
 G = np.load(Path(__file__).parent / "golden" / "reference_golden.npz")
@@ -189,6 +189,25 @@ def test_bit_identical_to_reference_gpu_cornell(tail, wide):
     assert ours.image().tobytes() == ref.image().tobytes()
     assert ours.rays_traced() == ref.stats()[2]
     ref.close()
+
+
+@pytest.mark.parametrize("depth", [8, 12])
+def test_bit_identical_to_patched_reference_at_depth(depth):
+    """The configs quoted at bounce limits 8 and 12 against the "patched reference" (the same
+    renderer sources with the literal 50 set to that depth): the same bits, on the Cornell box and
+    a small procedural scene, MIS and classic lighting."""
+    if not ref_gpu_so(depth).exists():
+        pytest.skip("patched reference build absent")
+    scenes = [pt.cornell_box(64, 40), pt.procedural_scene(48, 30, sphere_count=3, segments=48, rings=25, seed=4)]
+    for (s, cam), mis in zip(scenes, (True, False)):
+        w, h = (64, 40) if len(s.spheres) else (48, 30)
+        ref = RefGpu(depth).renderer(s, cam, w, h, 3, mis=mis)
+        ref.add_samples(5)
+        ours = pt.CudaRenderer(s, cam, w, h, 3, direct_light=mis, max_depth=depth)
+        ours.add_samples(5)
+        assert ours.image().tobytes() == ref.image().tobytes()
+        assert ours.rays_traced() == ref.stats()[2]
+        ref.close()
 
 
 @pytest.mark.parametrize("tail", [0, 2**31 - 1], ids=["wavefront", "fused"])
