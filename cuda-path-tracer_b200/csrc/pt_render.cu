@@ -38,8 +38,8 @@ struct RenderBuffers {
     ShadowRay *shadows;
     int32_t *queue[2];
     int32_t *shadow_queue;
-    int32_t *counters;      // [0],[1]: path queues; [2]: shadow queue
-    unsigned long long *fetch;   // [0]: extend's item counter, [1]: shadow's item counter
+    int32_t *counters;      // [0],[1]: path queues; [2],[3]: shadow queues of even and odd iterations
+    unsigned long long *fetch;   // [0]: extend's item counter, [1],[2]: the shadow kernels' item counters
     unsigned long long *rays;
     int32_t *error;
     float *sums;
@@ -62,7 +62,10 @@ __global__ void init_pixels(float *sums, Pcg *rng, int32_t count, uint64_t seed)
 // First camera ray of every pixel; queue 0 = all pixels in order.
 __global__ void start_samples(RenderParams p, RenderBuffers b, int32_t count, int samples) {
     int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i == 0) { b.counters[0] = count; b.counters[1] = 0; b.counters[2] = 0; b.fetch[0] = 0; b.fetch[1] = 0; }
+    if (i == 0) {
+        b.counters[0] = count; b.counters[1] = 0; b.counters[2] = 0; b.counters[3] = 0;
+        b.fetch[0] = 0; b.fetch[1] = 0; b.fetch[2] = 0;
+    }
     if (i >= count) return;
     Pcg rng = b.rng[i];
     PathState s;
@@ -79,8 +82,10 @@ __global__ void extend_kernel(DeviceScene scene, RenderParams p, RenderBuffers b
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         atomicAdd(b.rays, (unsigned long long)n);
         b.counters[parity ^ 1] = 0;      // the next queue fills during shade
-        b.counters[2] = 0;
-        b.fetch[1] = 0;                  // the shadow kernel's item counter
+        // this iteration's shadow slot (the previous iteration's shadow kernel, which may still
+        // be running on the other stream, uses the other slot)
+        b.counters[2 + parity] = 0;
+        b.fetch[1 + parity] = 0;
     }
     const int32_t *queue = b.queue[parity];
     if (!p.brute && p.debug != PT_DEBUG_BVH && p.debug != PT_DEBUG_INTERSECTIONS) {
@@ -146,7 +151,7 @@ __global__ void shade_kernel(DeviceScene scene, RenderParams p, RenderBuffers b,
             if (shadow) b.shadows[i] = sr;
         }
         push(live, i, out, &b.counters[parity ^ 1]);
-        push(shadow, i, b.shadow_queue, &b.counters[2]);
+        push(shadow, i, b.shadow_queue, &b.counters[2 + parity]);
     }
 }
 
@@ -204,8 +209,8 @@ __global__ void finish_kernel(DeviceScene scene, RenderParams p, RenderBuffers b
 }
 
 // shadow: any-hit of the NEE rays (transport.h:206-214); unoccluded ones add their contribution
-__global__ void shadow_kernel(DeviceScene scene, RenderParams p, RenderBuffers b, int min_active) {
-    const int32_t n = b.counters[2];
+__global__ void shadow_kernel(DeviceScene scene, RenderParams p, RenderBuffers b, int parity, int min_active) {
+    const int32_t n = b.counters[2 + parity];
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(b.rays, (unsigned long long)n);
     auto add = [&](int32_t i, const ShadowRay &sr) {
         PathState &s = b.paths[i];
@@ -223,9 +228,9 @@ __global__ void shadow_kernel(DeviceScene scene, RenderParams p, RenderBuffers b
             if (w.error) { *b.error = 1; return; }
             if (w.slot < 0) { int32_t i = b.shadow_queue[k]; add(i, b.shadows[i]); }
         };
-        if (p.wide == 2) persistent_walk4_spec<true>(scene, size_t(n), &b.fetch[1], min_active, kTieLastLeaf, get, done);
-        else if (p.wide) persistent_walk4<true>(scene, size_t(n), &b.fetch[1], min_active, kTieLastLeaf, get, done);
-        else persistent_walk<true>(scene, size_t(n), &b.fetch[1], min_active, kTieLastLeaf, get, done);
+        if (p.wide == 2) persistent_walk4_spec<true>(scene, size_t(n), &b.fetch[1 + parity], min_active, kTieLastLeaf, get, done);
+        else if (p.wide) persistent_walk4<true>(scene, size_t(n), &b.fetch[1 + parity], min_active, kTieLastLeaf, get, done);
+        else persistent_walk<true>(scene, size_t(n), &b.fetch[1 + parity], min_active, kTieLastLeaf, get, done);
         return;
     }
     for (int32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
@@ -282,11 +287,14 @@ struct pt_renderer {
     DeviceBuffer paths, hits, stats, shadows, queue0, queue1, shadow_queue, counters, fetch, ray_total, error, sums, rng, rgba;
     RenderBuffers buf{};
     cudaStream_t stream = nullptr;
+    cudaStream_t shadow_stream = nullptr;   // shadow kernel k runs beside extend k+1
     Event start, stop;
+    Event shaded[2], shadowed[2];           // by iteration parity
     int32_t *host_counters = nullptr;   // pinned, one slot per in-flight iteration
     Event iteration_events[8];
     ~pt_renderer() {
         if (host_counters) cudaFreeHost(host_counters);
+        if (shadow_stream) cudaStreamDestroy(shadow_stream);
         if (stream) cudaStreamDestroy(stream);
     }
     void grids() {
@@ -342,7 +350,7 @@ pt_status pt_renderer_create(const pt_scene *scene, const pt_camera *camera, int
             r->queue1.resize(n * sizeof(int32_t));
             r->shadow_queue.resize(n * sizeof(int32_t));
             r->counters.resize(4 * sizeof(int32_t));
-            r->fetch.resize(2 * sizeof(unsigned long long));
+            r->fetch.resize(3 * sizeof(unsigned long long));
             r->ray_total.resize(sizeof(unsigned long long));
             r->error.resize(sizeof(int32_t));
             r->sums.resize(n * 3 * sizeof(float));
@@ -356,6 +364,7 @@ pt_status pt_renderer_create(const pt_scene *scene, const pt_camera *camera, int
             b.rays = r->ray_total.get<unsigned long long>(); b.error = r->error.get<int32_t>();
             b.sums = r->sums.get<float>(); b.rng = r->rng.get<Pcg>();
             PT_CUDA(cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking));
+            PT_CUDA(cudaStreamCreateWithFlags(&r->shadow_stream, cudaStreamNonBlocking));
             PT_CUDA(cudaMallocHost(&r->host_counters, kIterationRing * sizeof(int32_t)));
             r->grids();
             r->tail_paths = std::max<int32_t>(16384, r->pixels / 16);
@@ -395,14 +404,22 @@ pt_status pt_add_samples(pt_renderer *r, int count) {
         PT_CUDA(cudaGetLastError());
         // Every pixel needs at most count * (max_depth + 1) extends; the loop ends earlier when
         // the queue is empty.  The queue length is read back with a lag of a few iterations.
+        // Iteration k: extend k and shade k on the main stream, shadow k on the shadow stream
+        // after shade k; shade k+1 waits for shadow k (it rewrites the shadow records and reads
+        // the radiance shadow k adds), so shadow k overlaps extend k+1 only.
         const int64_t max_iterations = int64_t(count) * (int64_t(r->params.max_depth) + 1) + 1;
         int parity = 0;
         int64_t issued = 0, checked = 0;
         bool done = false, tail = false;
         while (!done && !tail && issued < max_iterations) {
             extend_kernel<<<r->grid_extend, r->block, stack_bytes(r->block), st>>>(scene, r->params, r->buf, parity, g_query_config.min_active);
+            if (issued > 0) PT_CUDA(cudaStreamWaitEvent(st, r->shadowed[parity ^ 1].get(), 0));
             shade_kernel<<<r->grid_shade, r->block, 0, st>>>(scene, r->params, r->buf, parity);
-            shadow_kernel<<<r->grid_shadow, r->block, stack_bytes(r->block), st>>>(scene, r->params, r->buf, g_query_config.min_active);
+            PT_CUDA(cudaEventRecord(r->shaded[parity].get(), st));
+            PT_CUDA(cudaStreamWaitEvent(r->shadow_stream, r->shaded[parity].get(), 0));
+            shadow_kernel<<<r->grid_shadow, r->block, stack_bytes(r->block), r->shadow_stream>>>(scene, r->params, r->buf, parity,
+                                                                                                  g_query_config.min_active);
+            PT_CUDA(cudaEventRecord(r->shadowed[parity].get(), r->shadow_stream));
             PT_CUDA(cudaGetLastError());
             parity ^= 1;
             int slot = int(issued % kIterationRing);
@@ -419,6 +436,8 @@ pt_status pt_add_samples(pt_renderer *r, int count) {
                 checked++;
             }
         }
+        // the last shadow kernel joins the main stream
+        if (issued > 0) PT_CUDA(cudaStreamWaitEvent(st, r->shadowed[parity ^ 1].get(), 0));
         if (tail && !done) {
             // the few remaining paths (of the last issued iteration's queue) run to completion
             finish_kernel<<<r->grid_finish, r->block, 0, st>>>(scene, r->params, r->buf, parity);
