@@ -367,7 +367,7 @@ pt_status pt_renderer_create(const pt_scene *scene, const pt_camera *camera, int
             PT_CUDA(cudaStreamCreateWithFlags(&r->shadow_stream, cudaStreamNonBlocking));
             PT_CUDA(cudaMallocHost(&r->host_counters, kIterationRing * sizeof(int32_t)));
             r->grids();
-            r->tail_paths = std::max<int32_t>(16384, r->pixels / 16);
+            r->tail_paths = std::max<int32_t>(16384, r->pixels / 8);
         } catch (...) { delete r; throw; }
         *out = r;
         pt_status st = pt_reset(r, camera);
