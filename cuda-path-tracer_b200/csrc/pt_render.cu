@@ -77,7 +77,7 @@ __global__ void start_samples(RenderParams p, RenderBuffers b, int32_t count, in
 }
 
 // extend: closest hit of each queued path (trace_color's trace_world, transport.h:177-178)
-__global__ void extend_kernel(DeviceScene scene, RenderParams p, RenderBuffers b, int parity, int min_active) {
+__global__ void __launch_bounds__(256, 4) extend_kernel(DeviceScene scene, RenderParams p, RenderBuffers b, int parity, int min_active) {
     const int32_t n = b.counters[parity];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         atomicAdd(b.rays, (unsigned long long)n);
@@ -129,7 +129,7 @@ __device__ inline ShadeCtx shade_ctx(const RenderParams &p) {
 }
 
 // shade: shade_path over the queue; live paths and shadow rays are appended (warp-aggregated)
-__global__ void shade_kernel(DeviceScene scene, RenderParams p, RenderBuffers b, int parity) {
+__global__ void __launch_bounds__(256, 4) shade_kernel(DeviceScene scene, RenderParams p, RenderBuffers b, int parity) {
     const int32_t n = b.counters[parity];
     const int32_t *in = b.queue[parity];
     int32_t *out = b.queue[parity ^ 1];
@@ -209,7 +209,7 @@ __global__ void finish_kernel(DeviceScene scene, RenderParams p, RenderBuffers b
 }
 
 // shadow: any-hit of the NEE rays (transport.h:206-214); unoccluded ones add their contribution
-__global__ void shadow_kernel(DeviceScene scene, RenderParams p, RenderBuffers b, int parity, int min_active) {
+__global__ void __launch_bounds__(256, 4) shadow_kernel(DeviceScene scene, RenderParams p, RenderBuffers b, int parity, int min_active) {
     const int32_t n = b.counters[2 + parity];
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(b.rays, (unsigned long long)n);
     auto add = [&](int32_t i, const ShadowRay &sr) {
