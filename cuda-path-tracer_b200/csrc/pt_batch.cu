@@ -50,8 +50,8 @@ struct BatchBuffers {
     int32_t *slot_job;
     int32_t *queue[2];
     int32_t *shadow_queue;
-    int32_t *counters;                // [0],[1] path queues, [2] shadow queue
-    unsigned long long *fetch;        // [0] extend items, [1] shadow items
+    int32_t *counters;                // [0],[1] path queues, [2],[3] shadow queues of even and odd iterations
+    unsigned long long *fetch;        // [0] extend items, [1],[2] shadow items of even and odd iterations
     unsigned long long *cursor;       // next pixel to start
     unsigned long long *rays;
     int32_t *job_remaining;
@@ -117,8 +117,8 @@ __device__ inline void start_pixel(const BatchBuffers &b, int32_t slot, int64_t 
 __global__ void batch_start(BatchBuffers b, int32_t slots) {
     int32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k == 0) {
-        b.counters[0] = slots; b.counters[1] = 0; b.counters[2] = 0;
-        b.fetch[0] = 0; b.fetch[1] = 0;
+        b.counters[0] = slots; b.counters[1] = 0; b.counters[2] = 0; b.counters[3] = 0;
+        b.fetch[0] = 0; b.fetch[1] = 0; b.fetch[2] = 0;
         *b.cursor = (unsigned long long)slots;
         *b.start_ns = globaltimer();
         *b.iterations = 0;
@@ -136,8 +136,8 @@ __global__ void batch_extend(DeviceScene scene, BatchBuffers b, int parity, int 
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         atomicAdd(b.rays, (unsigned long long)n);
         b.counters[parity ^ 1] = 0;
-        b.counters[2] = 0;
-        b.fetch[1] = 0;
+        b.counters[2 + parity] = 0;      // this iteration's shadow slot (the other may be in use)
+        b.fetch[1 + parity] = 0;
     }
     const int32_t *queue = b.queue[parity];
     auto get = [&](size_t k, pt_ray &r, float &lo, float &hi, int32_t &root) {
@@ -198,12 +198,12 @@ __global__ void batch_shade(DeviceScene scene, BatchBuffers b, int parity) {
         }
         if (valid) b.paths[slot] = s;
         push(live, slot, out, &b.counters[parity ^ 1]);
-        push(shadow, slot, b.shadow_queue, &b.counters[2]);
+        push(shadow, slot, b.shadow_queue, &b.counters[2 + parity]);
     }
 }
 
-__global__ void batch_shadow(DeviceScene scene, BatchBuffers b, int min_active) {
-    const int32_t n = b.counters[2];
+__global__ void batch_shadow(DeviceScene scene, BatchBuffers b, int parity, int min_active) {
+    const int32_t n = b.counters[2 + parity];
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(b.rays, (unsigned long long)n);
     auto get = [&](size_t k, pt_ray &r, float &lo, float &hi, int32_t &root) {
         int32_t slot = b.shadow_queue[k];
@@ -223,7 +223,7 @@ __global__ void batch_shadow(DeviceScene scene, BatchBuffers b, int min_active) 
             s.rr = s.rr + sr.cr; s.rg = s.rg + sr.cg; s.rb = s.rb + sr.cb;
         }
     };
-    persistent_walk4_spec<true, true>(scene, size_t(n), &b.fetch[1], min_active, kTieLastLeaf, get, done);
+    persistent_walk4_spec<true, true>(scene, size_t(n), &b.fetch[1 + parity], min_active, kTieLastLeaf, get, done);
 }
 
 // One thread: continue the WHILE loop while paths are live, unless only a short tail is left
@@ -307,6 +307,8 @@ struct pt_batch {
     int32_t slots = 0;
     BatchBuffers buf{};
     cudaStream_t stream = nullptr;
+    cudaStream_t shadow_stream = nullptr;   // a shadow kernel runs beside the next extend
+    Event shaded[2], shadowed[2];
     cudaGraphExec_t exec = nullptr;
     cudaGraph_t graph = nullptr;
     Event start, stop;
@@ -316,6 +318,7 @@ struct pt_batch {
     ~pt_batch() {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
+        if (shadow_stream) cudaStreamDestroy(shadow_stream);
         if (stream) cudaStreamDestroy(stream);
     }
     void drop_graph() {
@@ -348,11 +351,22 @@ struct pt_batch {
         unsigned long long waves = (unsigned long long)((total_pixels + slots - 1) / std::max(slots, 1)) + 1;
         return worst * waves + 16;
     }
-    void iteration(int parity, cudaStream_t st) {
+    // Two wavefront iterations.  The first one's shadow kernel runs on the shadow stream beside
+    // the second one's extend; shade waits for the shadow kernel before it (it rewrites the
+    // shadow records and reads the radiance the shadow kernel adds); the pair ends joined.
+    void pair(cudaStream_t st) {
         const size_t smem = stack_smem();
-        batch_extend<true><<<grid((const void *)batch_extend<true>, smem), block, smem, st>>>(view, buf, parity, min_active);
-        batch_shade<<<grid((const void *)batch_shade, 0), block, 0, st>>>(view, buf, parity);
-        batch_shadow<<<grid((const void *)batch_shadow, smem), block, smem, st>>>(view, buf, min_active);
+        for (int parity = 0; parity < 2; parity++) {
+            batch_extend<true><<<grid((const void *)batch_extend<true>, smem), block, smem, st>>>(view, buf, parity, min_active);
+            if (parity == 1) PT_CUDA(cudaStreamWaitEvent(st, shadowed[0].get(), 0));
+            batch_shade<<<grid((const void *)batch_shade, 0), block, 0, st>>>(view, buf, parity);
+            PT_CUDA(cudaEventRecord(shaded[parity].get(), st));
+            PT_CUDA(cudaStreamWaitEvent(shadow_stream, shaded[parity].get(), 0));
+            batch_shadow<<<grid((const void *)batch_shadow, smem), block, smem, shadow_stream>>>(view, buf, parity, min_active);
+            PT_CUDA(cudaEventRecord(shadowed[parity].get(), shadow_stream));
+        }
+        PT_CUDA(cudaStreamWaitEvent(st, shadowed[1].get(), 0));
+        PT_CUDA(cudaGetLastError());
     }
     void build_graph() {
         drop_graph();
@@ -368,8 +382,7 @@ struct pt_batch {
         PT_CUDA(cudaGraphAddNode(&loop, graph, nullptr, 0, &cp));
         cudaGraph_t body = cp.conditional.phGraph_out[0];
         PT_CUDA(cudaStreamBeginCaptureToGraph(stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
-        iteration(0, stream);
-        iteration(1, stream);
+        pair(stream);
         batch_control<<<1, 32, 0, stream>>>(buf, handle, tail_paths, max_iterations());
         PT_CUDA(cudaStreamEndCapture(stream, &body));
         PT_CUDA(cudaStreamBeginCaptureToGraph(stream, graph, &loop, nullptr, 1, cudaStreamCaptureModeRelaxed));
@@ -400,8 +413,7 @@ struct pt_batch {
             PT_CUDA(cudaMallocHost(&live_host, 2 * sizeof(int64_t)));
             unsigned long long cursor = 0;
             for (unsigned long long it = 0;; it++) {
-                iteration(0, st);
-                iteration(1, st);
+                pair(st);
                 PT_CUDA(cudaMemcpyAsync(live_host, buf.counters, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
                 PT_CUDA(cudaMemcpyAsync(&cursor, buf.cursor, sizeof cursor, cudaMemcpyDeviceToHost, st));
                 PT_CUDA(cudaStreamSynchronize(st));
@@ -562,7 +574,7 @@ pt_status pt_batch_create(const pt_scene_desc *scenes, int32_t scene_count, cons
             b->sums.resize(size_t(offset) * 3 * sizeof(float));
             b->rng.resize(size_t(offset) * sizeof(Pcg));
             b->counters.resize(4 * sizeof(int32_t));
-            b->fetch.resize(2 * sizeof(unsigned long long));
+            b->fetch.resize(3 * sizeof(unsigned long long));
             b->scalars.resize(8 * sizeof(unsigned long long));
             b->job_remaining.resize(size_t(job_count) * sizeof(int32_t));
             b->job_done_ns.resize(size_t(job_count) * sizeof(unsigned long long));
@@ -577,6 +589,7 @@ pt_status pt_batch_create(const pt_scene_desc *scenes, int32_t scene_count, cons
             f.error = b->error.get<int32_t>();
             b->tail_paths = int32_t(std::max<int64_t>(16384, offset / 64));
             PT_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+            PT_CUDA(cudaStreamCreateWithFlags(&b->shadow_stream, cudaStreamNonBlocking));
             b->allocate_slots();
         } catch (...) { delete b; throw; }
         *out = b;
