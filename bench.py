@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--ref-spp", type=int, default=65536,
                     help="cache workload: samples of the FP64 reference image (0: time cached frames only)")
     ap.add_argument("--max-spp", type=int, default=4096, help="cache workload: sample budget of each curve")
+    ap.add_argument("--bvh", choices=["sah", "lbvh"], default="sah",
+                    help="query and batch48 workloads: the host binned-SAH tree (default) or the linear BVH built on the GPU")
     ap.add_argument("--no-graph", action="store_true",
                     help="cache frames: launch the kernels one by one instead of one graph per frame (for profilers)")
     return ap.parse_args()
@@ -175,7 +177,7 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def batch_jobs(count: int):
+def batch_jobs(count: int, gpu_bvh: bool = False):
     """Seeded render jobs 1..count: log-uniform 10k-2M triangles and 256x256-1920x1080 pixels,
     8-64 spp, bounce limit 4-12, scenes in the style of the procedural 1M-triangle scene."""
     scenes, jobs = [], []
@@ -188,7 +190,8 @@ def batch_jobs(count: int):
         h = int(min(1080, max(256, round(area / w))))
         spheres = int(min(30, max(1, round(tris / 65536))))
         seg = int(max(8, round(np.sqrt(tris / spheres))))
-        scene, cam = pt.procedural_scene(w, h, sphere_count=spheres, segments=seg, rings=max(3, seg // 2 + 1), seed=i)
+        scene, cam = pt.procedural_scene(w, h, sphere_count=spheres, segments=seg, rings=max(3, seg // 2 + 1), seed=i,
+                                         gpu_bvh=int(gpu_bvh))
         scenes.append(scene)
         jobs.append(dict(scene=i - 1, camera=cam, width=w, height=h, samples=int(g.integers(8, 65)),
                          max_depth=int(g.integers(4, 13)), seed=i))
@@ -200,7 +203,7 @@ def run_batch(args):
     import torch
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     t = time.perf_counter()
-    scenes, jobs = batch_jobs(args.jobs)
+    scenes, jobs = batch_jobs(args.jobs, gpu_bvh=args.bvh == "lbvh")
     build_s = time.perf_counter() - t
     b = pt.Batch(scenes, jobs)
     best = b.autotune(probe_samples=1, cache_path=None)
@@ -219,6 +222,7 @@ def run_batch(args):
                        "samples": int(sum(j["width"] * j["height"] * j["samples"] for j in jobs)),
                        "autotuned": {"path_capacity": best[0], "block": best[1], "min_active": best[2], "graph": best[3]}},
             "rays": rays, "job_completion_ms": [round(float(x), 3) for x in done], "scene_build_s": build_s,
+            "bvh": args.bvh,
             "clocks": clock}
     print(json.dumps(line), flush=True)
 
@@ -577,6 +581,11 @@ def main():
         return float(t.item())
 
     scene, cam, t_scene = build_scene()
+    t_gpu_build = None
+    if args.bvh == "lbvh":
+        t = time.perf_counter()
+        scene = scene.build_bvh(gpu=True)
+        t_gpu_build = time.perf_counter() - t
     dev = pt.Scene(scene)
     n_each = 1 << (args.log2_rays - 1)
     n = 2 * n_each
@@ -688,7 +697,7 @@ def main():
                    "bvh_nodes": int(len(scene.nodes)), "image": f"{WIDTH}x{HEIGHT}", "l2": "inputs larger than L2 (940 MB rays)",
                    "parallelism": f"replicas x{world}"},
         "kernel_ms": kernel_ms, "kernel_stats_per_ray": {"child_boxes": stats[0], "primitives": stats[1]},
-        "hit_rate": hit_rate, "scene_build_s": t_scene,
+        "hit_rate": hit_rate, "scene_build_s": t_scene, "bvh": args.bvh, "gpu_bvh_build_s": t_gpu_build,
         "clocks": clock, "gpu_launches": args.steps,
         "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
     }

@@ -181,39 +181,44 @@ private:
 
 } // namespace
 
-void build_sah(FlatScene &scene, int threads) {
-    std::vector<Prim> prims;
+std::vector<BuildPrim> gather_prims(const FlatScene &scene) {
+    std::vector<BuildPrim> prims;
     prims.reserve(scene.triangles.size() + scene.spheres.size());
     for(size_t i = 0; i < scene.triangles.size(); i++) {
-        Prim p; p.box = triangle_box(scene.triangles[i]); p.type = PT_TRIANGLE; p.id = int32_t(i);
-        for(int a = 0; a < 3; a++) p.centroid[a] = 0.5f*(p.box.lo[a] + p.box.hi[a]);
+        Box b = triangle_box(scene.triangles[i]);
+        BuildPrim p{}; p.type = PT_TRIANGLE; p.id = int32_t(i);
+        for(int a = 0; a < 3; a++) { p.lo[a] = b.lo[a]; p.hi[a] = b.hi[a]; }
         prims.push_back(p);
     }
     for(size_t i = 0; i < scene.spheres.size(); i++) {
-        Prim p; p.box = sphere_box(scene.spheres[i]); p.type = PT_SPHERE; p.id = int32_t(i);
-        for(int a = 0; a < 3; a++) p.centroid[a] = 0.5f*(p.box.lo[a] + p.box.hi[a]);
+        Box b = sphere_box(scene.spheres[i]);
+        BuildPrim p{}; p.type = PT_SPHERE; p.id = int32_t(i);
+        for(int a = 0; a < 3; a++) { p.lo[a] = b.lo[a]; p.hi[a] = b.hi[a]; }
         prims.push_back(p);
     }
     if(prims.size() >= size_t(INT32_MAX)/2) throw Error(PT_INVALID_ARGUMENT, "too many primitives for 32-bit node ids");
-    Builder builder(prims, threads < 1 ? hardware_threads() : threads);
-    int32_t root = builder.run();
+    return prims;
+}
+
+void export_preorder(FlatScene &scene, const std::vector<BuildNode> &nodes, int32_t root) {
     scene.nodes.clear();
     scene.max_depth = 0;
     if(root < 0) { scene.root = -1; return; }
     // preorder export, as flat_exporter::object emits nodes (src/flat/flat_export.h:100-114)
-    scene.nodes.reserve(builder.nodes_.size());
+    scene.nodes.reserve(nodes.size());
     struct Item { int32_t temp; int depth; int32_t parent; int side; };
     std::vector<Item> stack{{root, 1, -1, 0}};
     while(!stack.empty()) {
         Item it = stack.back(); stack.pop_back();
-        const TNode &t = builder.nodes_[size_t(it.temp)];
+        const BuildNode &t = nodes[size_t(it.temp)];
         int32_t id = int32_t(scene.nodes.size());
         pt_node n{};
-        n.minimum = {t.box.lo[0], t.box.lo[1], t.box.lo[2]};
-        n.maximum = {t.box.hi[0], t.box.hi[1], t.box.hi[2]};
+        n.minimum = {t.lo[0], t.lo[1], t.lo[2]};
+        n.maximum = {t.hi[0], t.hi[1], t.hi[2]};
         n.type = t.type; n.left = -1; n.right = -1; n.primitive = t.type == PT_BRANCH ? -1 : t.prim;
         scene.nodes.push_back(n);
         scene.max_depth = std::max(scene.max_depth, it.depth);
+        if(scene.max_depth > kStackCapacity) throw Error(PT_INVALID_ARGUMENT, "BVH deeper than 64 levels");
         if(it.parent >= 0) {
             if(it.side == 0) scene.nodes[size_t(it.parent)].left = id;
             else scene.nodes[size_t(it.parent)].right = id;
@@ -223,8 +228,29 @@ void build_sah(FlatScene &scene, int threads) {
             stack.push_back({t.left, it.depth + 1, id, 0});
         }
     }
-    if(scene.max_depth > kStackCapacity) throw Error(PT_INVALID_ARGUMENT, "BVH deeper than 64 levels");
     scene.root = 0;
+}
+
+void build_sah(FlatScene &scene, int threads) {
+    std::vector<BuildPrim> gathered = gather_prims(scene);
+    std::vector<Prim> prims;
+    prims.reserve(gathered.size());
+    for(const BuildPrim &g : gathered) {
+        Prim p;
+        for(int a = 0; a < 3; a++) { p.box.lo[a] = g.lo[a]; p.box.hi[a] = g.hi[a]; p.centroid[a] = 0.5f*(g.lo[a] + g.hi[a]); }
+        p.type = g.type; p.id = g.id;
+        prims.push_back(p);
+    }
+    Builder builder(prims, threads < 1 ? hardware_threads() : threads);
+    int32_t root = builder.run();
+    std::vector<BuildNode> nodes(builder.nodes_.size());
+    for(size_t i = 0; i < nodes.size(); i++) {
+        const TNode &t = builder.nodes_[i];
+        BuildNode &n = nodes[i];
+        for(int a = 0; a < 3; a++) { n.lo[a] = t.box.lo[a]; n.hi[a] = t.box.hi[a]; }
+        n.left = t.left; n.right = t.right; n.type = t.type; n.prim = t.prim;
+    }
+    export_preorder(scene, nodes, root);
 }
 
 } // namespace ptb

@@ -54,6 +54,16 @@ struct FlatScene {
 // their order, so primitive ids are the caller's indices.
 void build_sah(FlatScene &scene, int threads);
 
+// Builder interchange: primitive bounds (the reference's padded triangle boxes, sphere boxes),
+// temporary nodes (children are indices into the same array) and the preorder export both
+// builders share (one primitive per leaf, depth <= 64).
+struct BuildPrim { float lo[3], hi[3]; int32_t type, id; };
+struct BuildNode { float lo[3], hi[3]; int32_t left, right, type, prim; };
+std::vector<BuildPrim> gather_prims(const FlatScene &scene);
+void export_preorder(FlatScene &scene, const std::vector<BuildNode> &nodes, int32_t root);
+// Linear BVH on the GPU (pt_lbvh.cu): Morton order of centroids, Karras's radix tree.
+void build_lbvh(FlatScene &scene);
+
 int hardware_threads();
 
 } // namespace ptb

@@ -296,7 +296,7 @@ pt_status pt_workload_procedural(const pt_procedural_params *p, int width, int h
             float y = float(1.2 * B), x0 = float(0.5 * B - side / 2), z0 = float(0.5 * B - side / 2);
             quad(s.triangles, v(x0, y, z0), v(float(side), 0, 0), v(0, 0, float(side)), lamp);   // -y
         }
-        build_sah(s, 0);
+        if(p->gpu_bvh) build_lbvh(s); else build_sah(s, 0);
         if(camera) {
             float from[3] = {float(0.5 * B), float(0.75 * B), float(-1.1 * B)};
             float at[3] = {float(0.5 * B), float(0.35 * B), float(0.5 * B)}, up[3] = {0, 1, 0};

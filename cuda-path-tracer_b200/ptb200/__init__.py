@@ -87,7 +87,8 @@ class ProceduralParams(C.Structure):
                 ("displacement", C.c_float), ("radius_min", C.c_float), ("radius_max", C.c_float),
                 ("floor", C.c_int), ("light_fraction", C.c_float), ("light_radiance", C.c_float),
                 ("metal_fraction", C.c_float), ("glass_fraction", C.c_float), ("seed", C.c_uint64),
-                ("random_triangles", C.c_int), ("soup_edge_min", C.c_float), ("soup_edge_max", C.c_float)]
+                ("random_triangles", C.c_int), ("soup_edge_min", C.c_float), ("soup_edge_max", C.c_float),
+                ("gpu_bvh", C.c_int)]
 
 
 _lib = None
@@ -128,6 +129,7 @@ def library() -> C.CDLL:
         "pt_procedural_defaults": (None, [P]),
         "pt_workload_procedural": (I, [P, I, I, P, P]),
         "pt_workload_obj": (I, [C.c_char_p, I, I, P, P, P, P, P, P, S]),
+        "pt_flat_build_bvh_gpu": (I, [P]),
         "pt_rays_camera": (I, [P, I, I, U64, U64, S, P]),
         "pt_rays_surface": (I, [P, U64, U64, S, P, P, I]),
         "pt_rays_bounce": (I, [P, P, P, S, U64, U64, P, I]),
@@ -234,14 +236,15 @@ class FlatScene:
         return FlatScene(self.triangles.copy(), self.spheres.copy(), self.nodes.copy(), self.materials.copy(),
                          self.textures.copy(), self.pixels.copy(), self.root, self.max_depth)
 
-    def build_bvh(self, threads: int = 0) -> "FlatScene":
-        """Replaces the nodes with the library's binned-SAH tree (pt_flat_build_bvh)."""
+    def build_bvh(self, threads: int = 0, gpu: bool = False) -> "FlatScene":
+        """Replaces the nodes with the library's binned-SAH tree (pt_flat_build_bvh), or with
+        the linear BVH built on the GPU (gpu=True, pt_flat_build_bvh_gpu)."""
         lib = library()
         h = C.c_void_p()
         d = self.desc()
         check(lib.pt_flat_from_desc(C.byref(d), C.byref(h)))
         try:
-            check(lib.pt_flat_build_bvh(h, threads))
+            check(lib.pt_flat_build_bvh_gpu(h) if gpu else lib.pt_flat_build_bvh(h, threads))
             return _flat_from_handle(h)
         finally:
             lib.pt_flat_destroy(h)

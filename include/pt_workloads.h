@@ -23,6 +23,12 @@ pt_status pt_flat_from_desc(const pt_scene_desc *desc, pt_flat **out);
 /* Replaces the node array with a binned-SAH tree over all triangles and spheres
  * (one primitive per leaf, preorder, padded triangle bounds, depth <= 64). threads <= 0: all. */
 pt_status pt_flat_build_bvh(pt_flat *scene, int threads);
+/* The same output as pt_flat_build_bvh, built on the GPU as a linear BVH: 63-bit Morton codes of
+ * the primitive box centroids, radix sort, the binary radix tree of the sorted codes built in
+ * parallel (Karras 2012), node boxes as unions of the children's.  Much faster to build for large
+ * scenes; the tree traverses somewhat slower than the SAH one.  Needs a CUDA device; fails with
+ * PT_INVALID_ARGUMENT if the tree would be deeper than 64 levels. */
+pt_status pt_flat_build_bvh_gpu(pt_flat *scene);
 /* Pointers into the scene's arrays (valid until pt_flat_destroy). */
 pt_status pt_flat_desc(const pt_flat *scene, pt_scene_desc *desc);
 pt_status pt_flat_destroy(pt_flat *scene);
@@ -52,6 +58,7 @@ typedef struct pt_procedural_params {
     uint64_t seed;
     int random_triangles;    /* extra uniformly placed small triangles (soup) */
     float soup_edge_min, soup_edge_max;
+    int gpu_bvh;             /* 0: binned-SAH tree built on the host; 1: linear BVH built on the GPU */
 } pt_procedural_params;
 void pt_procedural_defaults(pt_procedural_params *params);
 pt_status pt_workload_procedural(const pt_procedural_params *params, int width, int height,
