@@ -46,6 +46,8 @@ namespace nrc {
 
 constexpr int kMaxSuffix = 8;
 constexpr int kMaxSteps = 8;
+constexpr int kShadowSlot = 5 + kMaxSteps;   // counters[kShadowSlot + parity]: shadow queue of even / odd iterations
+constexpr int kCounters = kShadowSlot + 2;
 
 struct alignas(16) CachePath {
     float ox, oy, oz, time;
@@ -193,13 +195,13 @@ __device__ inline pt_ray cache_ray(const CachePath &s) {
     return r;
 }
 
-__global__ void extend_kernel(DeviceScene scene, Params p, Buffers b, int parity, int min_active) {
+__global__ void __launch_bounds__(256, 4) extend_kernel(DeviceScene scene, Params p, Buffers b, int parity, int min_active) {
     const int32_t n = b.counters[parity];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         atomicAdd(&b.totals[0], (unsigned long long)n);
         b.counters[parity ^ 1] = 0;
-        b.counters[2] = 0;
-        b.fetch[1] = 0;
+        b.counters[kShadowSlot + parity] = 0;   // this iteration's shadow slot (the other may be in use)
+        b.fetch[1 + parity] = 0;
     }
     const int32_t *queue = b.queue[parity];
     auto get = [&](size_t k, pt_ray &r, float &lo, float &hi) { r = cache_ray(b.paths[queue[k]]); lo = 0.001f; hi = FLT_MAX; };
@@ -405,7 +407,7 @@ __global__ void shade_kernel(DeviceScene scene, Params p, Buffers b, int parity)
             b.paths[i] = s;
         }
         push(live, i, out, &b.counters[parity ^ 1]);
-        push(o.shadow, i, b.shadow_queue, &b.counters[2]);
+        push(o.shadow, i, b.shadow_queue, &b.counters[kShadowSlot + parity]);
     }
 }
 
@@ -462,8 +464,8 @@ __global__ void finish_kernel(DeviceScene scene, Params p, Buffers b, int parity
     if ((threadIdx.x & 31) == 0 && rays) atomicAdd(&b.totals[0], rays);
 }
 
-__global__ void shadow_kernel(DeviceScene scene, Params p, Buffers b, int min_active) {
-    const int32_t n = b.counters[2];
+__global__ void __launch_bounds__(256, 4) shadow_kernel(DeviceScene scene, Params p, Buffers b, int parity, int min_active) {
+    const int32_t n = b.counters[kShadowSlot + parity];
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&b.totals[0], (unsigned long long)n);
     auto get = [&](size_t k, pt_ray &r, float &lo, float &hi) {
         const CacheShadow &sr = b.shadows[b.shadow_queue[k]];
@@ -481,9 +483,9 @@ __global__ void shadow_kernel(DeviceScene scene, Params p, Buffers b, int min_ac
         s.rr += sr.cr; s.rg += sr.cg; s.rb += sr.cb;
         if (sr.suffix) { s.sr += sr.sr; s.sg += sr.sg; s.sb += sr.sb; }
     };
-    if (p.wide == 2) persistent_walk4_spec<true>(scene, size_t(n), &b.fetch[1], min_active, kTieLastLeaf, get, done);
-    else if (p.wide) persistent_walk4<true>(scene, size_t(n), &b.fetch[1], min_active, kTieLastLeaf, get, done);
-    else persistent_walk<true>(scene, size_t(n), &b.fetch[1], min_active, kTieLastLeaf, get, done);
+    if (p.wide == 2) persistent_walk4_spec<true>(scene, size_t(n), &b.fetch[1 + parity], min_active, kTieLastLeaf, get, done);
+    else if (p.wide) persistent_walk4<true>(scene, size_t(n), &b.fetch[1 + parity], min_active, kTieLastLeaf, get, done);
+    else persistent_walk<true>(scene, size_t(n), &b.fetch[1 + parity], min_active, kTieLastLeaf, get, done);
 }
 
 // Pixel sums += weight x prediction of the pixel's queries, in sample order.
@@ -577,7 +579,8 @@ struct pt_cached_renderer {
     DeviceBuffer paths, hits, shadows, queue0, queue1, shadow_queue, counters, fetch, totals, error, sums, rng, frame;
     DeviceBuffer queries, aux, pred, pixel_queries, pixel_query_count, vertices, ends, samples, targets;
     Buffers buf{};
-    cudaStream_t stream = nullptr, body_stream = nullptr;
+    cudaStream_t stream = nullptr, body_stream = nullptr, shadow_stream = nullptr;
+    Event shaded[2], shadowed[2];
     Event start, stop;
     int32_t tail_paths = 0;             // live paths below which the fused kernel ends the frame
     int32_t *live_host = nullptr;       // pinned: live count read back by the launched form
@@ -589,6 +592,7 @@ struct pt_cached_renderer {
         if (cache) pt_cache_destroy(cache);
         if (live_host) cudaFreeHost(live_host);
         if (body_stream) cudaStreamDestroy(body_stream);
+        if (shadow_stream) cudaStreamDestroy(shadow_stream);
         if (stream) cudaStreamDestroy(stream);
     }
     // the launches of one frame (also what a graph captures)
@@ -605,18 +609,27 @@ struct pt_cached_renderer {
         return (unsigned long long)p.spf * (unsigned long long)(p.max_depth + 1) / 2 + 2;
     }
     void prologue(const Params &p, cudaStream_t st) {
-        PT_CUDA(cudaMemsetAsync(buf.counters, 0, (5 + kMaxSteps) * sizeof(int32_t), st));
-        PT_CUDA(cudaMemsetAsync(buf.fetch, 0, 2 * sizeof(unsigned long long), st));
+        PT_CUDA(cudaMemsetAsync(buf.counters, 0, kCounters * sizeof(int32_t), st));
+        PT_CUDA(cudaMemsetAsync(buf.fetch, 0, 3 * sizeof(unsigned long long), st));
         PT_CUDA(cudaMemsetAsync(buf.pairs, 0, sizeof(unsigned long long), st));
         start_kernel<<<(pixels + 255) / 256, 256, 0, st>>>(p, buf, pixels);
         PT_CUDA(cudaGetLastError());
     }
+    // Two iterations.  The first one's shadow kernel runs on the shadow stream beside the
+    // second one's extend; shade waits for the shadow kernel before it (it rewrites the shadow
+    // records and reads the radiance the shadow kernel adds); the pair ends joined.
     void iteration_pair(const Params &p, cudaStream_t st) {
         for (int parity = 0; parity < 2; parity++) {
             extend_kernel<<<grid_extend, block, stack_bytes(block), st>>>(scene->view, p, buf, parity, g_query_config.min_active);
+            if (parity == 1) PT_CUDA(cudaStreamWaitEvent(st, shadowed[0].get(), 0));
             shade_kernel<<<grid_shade, block, 0, st>>>(scene->view, p, buf, parity);
-            shadow_kernel<<<grid_shadow, block, stack_bytes(block), st>>>(scene->view, p, buf, g_query_config.min_active);
+            PT_CUDA(cudaEventRecord(shaded[parity].get(), st));
+            PT_CUDA(cudaStreamWaitEvent(shadow_stream, shaded[parity].get(), 0));
+            shadow_kernel<<<grid_shadow, block, stack_bytes(block), shadow_stream>>>(scene->view, p, buf, parity,
+                                                                                    g_query_config.min_active);
+            PT_CUDA(cudaEventRecord(shadowed[parity].get(), shadow_stream));
         }
+        PT_CUDA(cudaStreamWaitEvent(st, shadowed[1].get(), 0));
         PT_CUDA(cudaGetLastError());
     }
     // the fused kernel ends the paths left in queue 0, then the network's part of the frame
@@ -795,8 +808,8 @@ pt_status pt_cached_create(const pt_scene *scene, const pt_camera *camera, int w
             r->queue0.resize(n * sizeof(int32_t));
             r->queue1.resize(n * sizeof(int32_t));
             r->shadow_queue.resize(n * sizeof(int32_t));
-            r->counters.resize((5 + kMaxSteps) * sizeof(int32_t));
-            r->fetch.resize(2 * sizeof(unsigned long long));
+            r->counters.resize(kCounters * sizeof(int32_t));
+            r->fetch.resize(3 * sizeof(unsigned long long));
             r->totals.resize(3 * sizeof(unsigned long long));
             r->error.resize(sizeof(int32_t));
             r->sums.resize(n * 3 * sizeof(float));
@@ -830,6 +843,7 @@ pt_status pt_cached_create(const pt_scene *scene, const pt_camera *camera, int w
             b.samples = r->samples.get<pt_cache_query>(); b.targets = r->targets.get<float>();
             PT_CUDA(cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking));
             PT_CUDA(cudaStreamCreateWithFlags(&r->body_stream, cudaStreamNonBlocking));
+            PT_CUDA(cudaStreamCreateWithFlags(&r->shadow_stream, cudaStreamNonBlocking));
             PT_CUDA(cudaMallocHost(&r->live_host, sizeof(int32_t)));
             r->pairs.resize(sizeof(unsigned long long));
             b.pairs = r->pairs.get<unsigned long long>();
