@@ -232,17 +232,19 @@ struct Sync {
 };
 
 // ---- forward (query) -----------------------------------------------------------------------
-// smem: header | W (43008) | pad | X | pad | H | pad
-constexpr size_t kFwdSmem = 256 + kWeightBytes + kPad + 2 * (kActBytes + kPad);
+// smem: header | W (43008) | pad | X | pad.  One activation buffer: each layer's epilogue runs
+// after that layer's MMA has completed, so it overwrites the MMA's own input in place.  About
+// 62 KB a CTA, so three CTAs (three tiles in flight, 3 x 128 TMEM columns) share an SM.
+constexpr size_t kFwdSmem = 256 + kWeightBytes + kPad + (kActBytes + kPad);
+constexpr int kFwdCtasPerSm = 3;
 
-__global__ void __launch_bounds__(kTile, 1) forward_kernel(const unsigned char *weights, const pt_cache_query *queries, size_t count,
+__global__ void __launch_bounds__(kTile, kFwdCtasPerSm) forward_kernel(const unsigned char *weights, const pt_cache_query *queries, size_t count,
                                                            const int32_t *count_dev, float3 lo, float3 hi, float *out, int *status) {
     if (count_dev) count = min(count, size_t(max(0, *count_dev)));   // queue length known only on the device
     extern __shared__ __align__(1024) unsigned char smem[];
     Scratch *h = reinterpret_cast<Scratch *>(smem);
     unsigned char *w = smem + 256;
-    unsigned char *bufx = w + kWeightBytes + kPad;
-    unsigned char *bufh = bufx + kActBytes + kPad;
+    unsigned char *act = w + kWeightBytes + kPad;
     const float l[3] = {lo.x, lo.y, lo.z};
     const float ie[3] = {1.0f / fmaxf(hi.x - lo.x, 1e-30f), 1.0f / fmaxf(hi.y - lo.y, 1e-30f), 1.0f / fmaxf(hi.z - lo.z, 1e-30f)};
     if (threadIdx.x == 0) bar_init(&h->bar);
@@ -258,31 +260,29 @@ __global__ void __launch_bounds__(kTile, 1) forward_kernel(const unsigned char *
     bool ok = true;
     const size_t tiles = (count + kTile - 1) / kTile;
     for (size_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
-        encode_tile(bufx, queries, t * kTile, count, l, ie);
+        encode_tile(act, queries, t * kTile, count, l, ie);
         fence_async_smem();
         fence_before();
         __syncthreads();
         fence_after();
-        unsigned char *in = bufx, *outb = bufh;
         for (int layer = 0; layer < kHidden && ok; layer++) {
-            if (threadIdx.x == 0) mma_kk(tbase, in, 64, w + layer * kMatBytes, 64, 64, 64, false);
-            ok = sync.wait_all();
+            if (threadIdx.x == 0) mma_kk(tbase, act, 64, w + layer * kMatBytes, 64, 64, 64, false);
+            ok = sync.wait_all();        // the MMA has read all of act: its rows may be overwritten
             if (!ok) break;
             for (int c = 0; c < 4; c++) {
                 float v[16];
                 tmem_ld16(lane_base + c * 16, v);
                 for (int i = 0; i < 16; i++) v[i] = fmaxf(v[i], 0.0f);
-                store8(outb, threadIdx.x, 2 * c, 64, v);
-                store8(outb, threadIdx.x, 2 * c + 1, 64, v + 8);
+                store8(act, threadIdx.x, 2 * c, 64, v);
+                store8(act, threadIdx.x, 2 * c + 1, 64, v + 8);
             }
             fence_async_smem();
             fence_before();
             __syncthreads();
             fence_after();
-            unsigned char *tmp = in; in = outb; outb = tmp;
         }
         if (!ok) break;
-        if (threadIdx.x == 0) mma_kk(tbase + 64, in, 64, w + kHidden * kMatBytes, 64, kOutPad, 64, false);
+        if (threadIdx.x == 0) mma_kk(tbase + 64, act, 64, w + kHidden * kMatBytes, 64, kOutPad, 64, false);
         ok = sync.wait_all();
         if (!ok) break;
         float v[16];
@@ -564,7 +564,7 @@ void cache_bounds(const pt_cache *c, float lo[3], float hi[3]) {
 void cache_forward(pt_cache *c, const pt_cache_query *queries, size_t count, const int32_t *count_dev, float *rgb, cudaStream_t st) {
     size_t tiles = (count + kTile - 1) / kTile;
     if (!tiles) return;
-    int grid = int(std::min<size_t>(tiles, size_t(2 * c->ctas)));
+    int grid = int(std::min<size_t>(tiles, size_t(kFwdCtasPerSm) * size_t(c->ctas)));
     forward_kernel<<<grid, kTile, kFwdSmem, st>>>(c->inference(), queries, count, count_dev, lo3(c), hi3(c), rgb,
                                                    c->status.get<int>());
     PT_CUDA(cudaGetLastError());
