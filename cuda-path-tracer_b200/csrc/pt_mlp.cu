@@ -112,6 +112,15 @@ __device__ inline void store8(unsigned char *base, uint32_t r, uint32_t c8, uint
     v.z = *reinterpret_cast<uint32_t *>(&p2); v.w = *reinterpret_cast<uint32_t *>(&p3);
     *reinterpret_cast<uint4 *>(base + canon(r, c8 * 8, cols)) = v;
 }
+// store8 of max(x, 0): the conversion instruction applies the ReLU
+__device__ inline void store8_relu(unsigned char *base, uint32_t r, uint32_t c8, uint32_t cols, const float *x) {
+    uint4 v;
+    asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(v.x) : "f"(x[1]), "f"(x[0]));
+    asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(v.y) : "f"(x[3]), "f"(x[2]));
+    asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(v.z) : "f"(x[5]), "f"(x[4]));
+    asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(v.w) : "f"(x[7]), "f"(x[6]));
+    *reinterpret_cast<uint4 *>(base + canon(r, c8 * 8, cols)) = v;
+}
 __device__ inline void load8(const unsigned char *base, uint32_t r, uint32_t c8, uint32_t cols, float *x) {
     uint4 v = *reinterpret_cast<const uint4 *>(base + canon(r, c8 * 8, cols));
     const __nv_bfloat162 *p = reinterpret_cast<const __nv_bfloat162 *>(&v);
@@ -125,12 +134,13 @@ __device__ inline void encode(const pt_cache_query &q, const float lo[3], const 
     int k = 0;
     for (int a = 0; a < 3; a++) {
         float p = (pos[a] - lo[a]) * inv_extent[a];
-        float s = 3.14159265358979f * p;
-        for (int f = 0; f < 6; f++) {
-            float sn, cs;
-            sincosf(s, &sn, &cs);
+        float sn, cs;
+        sincosf(3.14159265358979f * p, &sn, &cs);
+        for (int f = 0; f < 6; f++) {          // frequencies 2^f pi p by the double-angle identities
             x[k++] = sn; x[k++] = cs;
-            s *= 2.0f;
+            float s2 = 2.0f * sn * cs;
+            cs = (cs - sn) * (cs + sn);
+            sn = s2;
         }
     }
     float dx = q.direction.x, dy = q.direction.y, dz = q.direction.z;
@@ -180,13 +190,14 @@ __device__ inline void load_weights(unsigned char *w, const unsigned char *g) {
 }
 
 // X (128 x 64, rows = queries) into the core-matrix layout; rows past `count` are zero.
+// `r` is the calling thread's row of the tile.
 __device__ inline void encode_tile(unsigned char *x, const pt_cache_query *q, size_t first, size_t count, const float lo[3],
-                                   const float inv_extent[3]) {
+                                   const float inv_extent[3], uint32_t r) {
     float v[64];
-    size_t row = first + threadIdx.x;
+    size_t row = first + r;
     if (row < count) encode(q[row], lo, inv_extent, v);
     else for (int i = 0; i < 64; i++) v[i] = 0.0f;
-    for (int c = 0; c < 8; c++) store8(x, threadIdx.x, c, 64, v + 8 * c);
+    for (int c = 0; c < 8; c++) store8(x, r, c, 64, v + 8 * c);
 }
 
 // D[128 x N] (+)= A[128 x K] * B[N x K]^T, A and B K-major in the core layout, K = 16 per MMA.
@@ -232,71 +243,104 @@ struct Sync {
 };
 
 // ---- forward (query) -----------------------------------------------------------------------
-// smem: header | W (43008) | pad | X | pad.  One activation buffer: each layer's epilogue runs
-// after that layer's MMA has completed, so it overwrites the MMA's own input in place.  About
-// 62 KB a CTA, so three CTAs (three tiles in flight, 3 x 128 TMEM columns) share an SM.
-constexpr size_t kFwdSmem = 256 + kWeightBytes + kPad + (kActBytes + kPad);
-constexpr int kFwdCtasPerSm = 3;
+// A CTA runs kFwdGroups independent tile pipelines ("groups" of four warps, one 128-query tile
+// each) over one shared copy of the weights.  Group g owns TMEM columns [64g, 64g + 64) (each
+// hidden layer's 128 x 64 accumulator, then the 128 x 16 output in the same columns), one
+// activation buffer, one mbarrier and named barrier 1 + g.  One activation buffer suffices: each
+// layer's epilogue runs after that layer's MMA has completed, so it overwrites the MMA's own input.
+// smem: header (Scratch, then the groups' mbarriers from byte 128) | W | pad | (act | pad) x G.
+// Two CTAs of three groups share an SM: six tiles in flight, 2 x 256 TMEM columns.
+constexpr int kFwdGroups = 3;
+constexpr int kFwdThreads = kFwdGroups * kTile;
+constexpr int kFwdCtasPerSm = 2;
+constexpr uint32_t kFwdTmemCols = 256;    // power of two >= 64 * kFwdGroups
+constexpr size_t kFwdSmem = 256 + kWeightBytes + kPad + kFwdGroups * (kActBytes + kPad);
+static_assert(64 * kFwdGroups <= kFwdTmemCols && kFwdCtasPerSm * kFwdTmemCols <= 512, "TMEM budget");
+static_assert(128 + 8 * kFwdGroups <= 256 && kFwdGroups < 16, "header and named-barrier budget");
 
-__global__ void __launch_bounds__(kTile, kFwdCtasPerSm) forward_kernel(const unsigned char *weights, const pt_cache_query *queries, size_t count,
-                                                           const int32_t *count_dev, float3 lo, float3 hi, float *out, int *status) {
+// named barrier over one group's 128 threads; returns whether every thread passed `ok`
+__device__ inline bool group_sync_and(int id, bool ok) {
+    uint32_t r;
+    asm volatile("{\n\t.reg .pred p, q;\n\tsetp.ne.b32 p, %1, 0;\n\t"
+                 "barrier.cta.red.and.pred q, %2, 128, p;\n\tselp.b32 %0, 1, 0, q;\n\t}\n"
+                 : "=r"(r) : "r"((uint32_t)ok), "r"(id) : "memory");
+    return r != 0;
+}
+
+__global__ void __launch_bounds__(kFwdThreads, kFwdCtasPerSm) forward_kernel(const unsigned char *weights,
+                                                                             const pt_cache_query *queries, size_t count,
+                                                                             const int32_t *count_dev, float3 lo, float3 hi,
+                                                                             float *out, int *status) {
     if (count_dev) count = min(count, size_t(max(0, *count_dev)));   // queue length known only on the device
     extern __shared__ __align__(1024) unsigned char smem[];
     Scratch *h = reinterpret_cast<Scratch *>(smem);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + 128);
     unsigned char *w = smem + 256;
-    unsigned char *act = w + kWeightBytes + kPad;
+    const int g = threadIdx.x / kTile;
+    const uint32_t r = threadIdx.x % kTile;                        // this thread's row of its group's tile
+    unsigned char *act = w + kWeightBytes + kPad + size_t(g) * (kActBytes + kPad);
     const float l[3] = {lo.x, lo.y, lo.z};
     const float ie[3] = {1.0f / fmaxf(hi.x - lo.x, 1e-30f), 1.0f / fmaxf(hi.y - lo.y, 1e-30f), 1.0f / fmaxf(hi.z - lo.z, 1e-30f)};
-    if (threadIdx.x == 0) bar_init(&h->bar);
-    tmem_alloc(h, 128);
+    if (threadIdx.x < kFwdGroups) bar_init(&bars[threadIdx.x]);
+    tmem_alloc(h, kFwdTmemCols);
     load_weights(w, weights);
     fence_async_smem();
     fence_before();
     __syncthreads();
     fence_after();
-    const uint32_t tbase = h->tmem;
-    const uint32_t lane_base = tbase + ((uint32_t)(threadIdx.x & ~31u) << 16);
-    Sync sync{h};
+    const uint32_t tcol = h->tmem + 64u * uint32_t(g);
+    const uint32_t lane_col = tcol + ((uint32_t)((r & ~31u)) << 16);   // warp (w % 4) reads lanes 32 (w % 4) ..
+    uint64_t *bar = &bars[g];
+    const bool issuer = r == 0;
+    uint32_t phase = 0;
     bool ok = true;
-    const size_t tiles = (count + kTile - 1) / kTile;
-    for (size_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
-        encode_tile(act, queries, t * kTile, count, l, ie);
+    auto wait_mma = [&]() {                       // commit this group's MMAs and wait for them (bounded)
+        if (issuer) commit(bar);
+        bool done = bar_wait(bar, phase);
+        phase ^= 1;
+        fence_after();
+        return done;
+    };
+    auto sync_group = [&](bool v) {
         fence_async_smem();
         fence_before();
-        __syncthreads();
+        bool all = group_sync_and(1 + g, v);
         fence_after();
+        return all;
+    };
+    const size_t tiles = (count + kTile - 1) / kTile;
+    const size_t stride = size_t(gridDim.x) * kFwdGroups;
+    for (size_t t = size_t(blockIdx.x) * kFwdGroups + g; t < tiles && ok; t += stride) {
+        encode_tile(act, queries, t * kTile, count, l, ie, r);
+        sync_group(true);
         for (int layer = 0; layer < kHidden && ok; layer++) {
-            if (threadIdx.x == 0) mma_kk(tbase, act, 64, w + layer * kMatBytes, 64, 64, 64, false);
-            ok = sync.wait_all();        // the MMA has read all of act: its rows may be overwritten
-            if (!ok) break;
-            for (int c = 0; c < 4; c++) {
-                float v[16];
-                tmem_ld16(lane_base + c * 16, v);
-                for (int i = 0; i < 16; i++) v[i] = fmaxf(v[i], 0.0f);
-                store8(act, threadIdx.x, 2 * c, 64, v);
-                store8(act, threadIdx.x, 2 * c + 1, 64, v + 8);
+            if (issuer) mma_kk(tcol, act, 64, w + layer * kMatBytes, 64, 64, 64, false);
+            bool done = wait_mma();               // the MMA has read all of act: its rows may be overwritten
+            if (done) {
+                for (int c = 0; c < 4; c++) {
+                    float v[16];
+                    tmem_ld16(lane_col + c * 16, v);
+                    store8_relu(act, r, 2 * c, 64, v);
+                    store8_relu(act, r, 2 * c + 1, 64, v + 8);
+                }
             }
-            fence_async_smem();
-            fence_before();
-            __syncthreads();
-            fence_after();
+            ok = sync_group(done);
         }
         if (!ok) break;
-        if (threadIdx.x == 0) mma_kk(tbase + 64, act, 64, w + kHidden * kMatBytes, 64, kOutPad, 64, false);
-        ok = sync.wait_all();
-        if (!ok) break;
-        float v[16];
-        tmem_ld16(lane_base + 64, v);
-        size_t row = t * kTile + threadIdx.x;
-        if (row < count) { out[3 * row] = expf(v[0]); out[3 * row + 1] = expf(v[1]); out[3 * row + 2] = expf(v[2]); }
-        fence_before();
-        __syncthreads();
-        fence_after();
+        if (issuer) mma_kk(tcol, act, 64, w + kHidden * kMatBytes, 64, kOutPad, 64, false);
+        bool done = wait_mma();
+        if (done) {
+            float v[16];
+            tmem_ld16(lane_col, v);
+            size_t row = t * kTile + r;
+            if (row < count) { out[3 * row] = expf(v[0]); out[3 * row + 1] = expf(v[1]); out[3 * row + 2] = expf(v[2]); }
+        }
+        ok = sync_group(done);                    // the next tile's MMAs write these TMEM columns again
     }
-    if (!ok && threadIdx.x == 0) atomicExch(status, int(PT_TIMEOUT));
+    if (!ok && r == 0) atomicExch(status, int(PT_TIMEOUT));
     fence_before();
     __syncthreads();
-    tmem_free(tbase, 128);
+    tmem_free(h->tmem, kFwdTmemCols);
 }
 
 // ---- training (forward + relative-L2 loss + backward) --------------------------------------
@@ -335,7 +379,7 @@ __global__ void __launch_bounds__(kTile, 1) train_kernel(const unsigned char *we
     const size_t tiles = (count + kTile - 1) / kTile;
     for (size_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
         const size_t row = t * kTile + threadIdx.x;
-        encode_tile(act[0], queries, t * kTile, count, l, ie);
+        encode_tile(act[0], queries, t * kTile, count, l, ie, threadIdx.x);
         fence_async_smem();
         fence_before();
         __syncthreads();
@@ -347,9 +391,8 @@ __global__ void __launch_bounds__(kTile, 1) train_kernel(const unsigned char *we
             for (int c = 0; c < 4; c++) {
                 float v[16];
                 tmem_ld16(lane_base + c * 16, v);
-                for (int i = 0; i < 16; i++) v[i] = fmaxf(v[i], 0.0f);
-                store8(act[layer + 1], threadIdx.x, 2 * c, 64, v);
-                store8(act[layer + 1], threadIdx.x, 2 * c + 1, 64, v + 8);
+                store8_relu(act[layer + 1], threadIdx.x, 2 * c, 64, v);
+                store8_relu(act[layer + 1], threadIdx.x, 2 * c + 1, 64, v + 8);
             }
             fence_async_smem();
             fence_before();
@@ -564,8 +607,8 @@ void cache_bounds(const pt_cache *c, float lo[3], float hi[3]) {
 void cache_forward(pt_cache *c, const pt_cache_query *queries, size_t count, const int32_t *count_dev, float *rgb, cudaStream_t st) {
     size_t tiles = (count + kTile - 1) / kTile;
     if (!tiles) return;
-    int grid = int(std::min<size_t>(tiles, size_t(kFwdCtasPerSm) * size_t(c->ctas)));
-    forward_kernel<<<grid, kTile, kFwdSmem, st>>>(c->inference(), queries, count, count_dev, lo3(c), hi3(c), rgb,
+    int grid = int(std::min<size_t>((tiles + kFwdGroups - 1) / kFwdGroups, size_t(kFwdCtasPerSm) * size_t(c->ctas)));
+    forward_kernel<<<grid, kFwdThreads, kFwdSmem, st>>>(c->inference(), queries, count, count_dev, lo3(c), hi3(c), rgb,
                                                    c->status.get<int>());
     PT_CUDA(cudaGetLastError());
 }
