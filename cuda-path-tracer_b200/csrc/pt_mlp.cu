@@ -128,16 +128,30 @@ __device__ inline void load8(const unsigned char *base, uint32_t r, uint32_t c8,
     for (int i = 0; i < 4; i++) { float2 f = __bfloat1622float2(p[i]); x[2 * i] = f.x; x[2 * i + 1] = f.y; }
 }
 
-// Input encoding of one query (see the file comment); 64 values, zero padded.
-__device__ inline void encode(const pt_cache_query &q, const float lo[3], const float inv_extent[3], float x[64]) {
-    const float pos[3] = {q.position.x, q.position.y, q.position.z};
+// Collects a row's encoded values eight at a time and stores each group of eight as soon as it is
+// complete, so a thread holds at most eight of its 64 inputs in registers.
+struct RowWriter {
+    unsigned char *base;
+    uint32_t r;
+    float buf[8];
     int k = 0;
+    __device__ __forceinline__ void operator()(float v) {
+        buf[k & 7] = v;
+        if ((++k & 7) == 0) store8(base, r, uint32_t(k / 8 - 1), 64, buf);
+    }
+};
+
+// Input encoding of one query (see the file comment); 64 values, zero padded.
+__device__ __forceinline__ void encode(const pt_cache_query &q, float3 lo, float3 inv_extent, RowWriter &put) {
+    const float p3[3] = {(q.position.x - lo.x) * inv_extent.x, (q.position.y - lo.y) * inv_extent.y,
+                         (q.position.z - lo.z) * inv_extent.z};
+#pragma unroll
     for (int a = 0; a < 3; a++) {
-        float p = (pos[a] - lo[a]) * inv_extent[a];
         float sn, cs;
-        sincosf(3.14159265358979f * p, &sn, &cs);
+        sincosf(3.14159265358979f * p3[a], &sn, &cs);
+#pragma unroll
         for (int f = 0; f < 6; f++) {          // frequencies 2^f pi p by the double-angle identities
-            x[k++] = sn; x[k++] = cs;
+            put(sn); put(cs);
             float s2 = 2.0f * sn * cs;
             cs = (cs - sn) * (cs + sn);
             sn = s2;
@@ -145,26 +159,27 @@ __device__ inline void encode(const pt_cache_query &q, const float lo[3], const 
     }
     float dx = q.direction.x, dy = q.direction.y, dz = q.direction.z;
     float xx = dx * dx, yy = dy * dy, zz = dz * dz;
-    x[k++] = 0.28209479177387814f;
-    x[k++] = -0.48860251190291987f * dy;
-    x[k++] = 0.48860251190291987f * dz;
-    x[k++] = -0.48860251190291987f * dx;
-    x[k++] = 1.0925484305920792f * dx * dy;
-    x[k++] = -1.0925484305920792f * dy * dz;
-    x[k++] = 0.31539156525252005f * (3.0f * zz - 1.0f);
-    x[k++] = -1.0925484305920792f * dx * dz;
-    x[k++] = 0.5462742152960396f * (xx - yy);
-    x[k++] = -0.5900435899266435f * dy * (3.0f * xx - yy);
-    x[k++] = 2.890611442640554f * dx * dy * dz;
-    x[k++] = -0.4570457994644658f * dy * (5.0f * zz - 1.0f);
-    x[k++] = 0.3731763325901154f * dz * (5.0f * zz - 3.0f);
-    x[k++] = -0.4570457994644658f * dx * (5.0f * zz - 1.0f);
-    x[k++] = 1.445305721320277f * dz * (xx - yy);
-    x[k++] = -0.5900435899266435f * dx * (xx - 3.0f * yy);
-    x[k++] = q.normal.x; x[k++] = q.normal.y; x[k++] = q.normal.z;
-    x[k++] = q.albedo.x; x[k++] = q.albedo.y; x[k++] = q.albedo.z;
-    x[k++] = q.roughness;
-    while (k < 64) x[k++] = 0.0f;
+    put(0.28209479177387814f);
+    put(-0.48860251190291987f * dy);
+    put(0.48860251190291987f * dz);
+    put(-0.48860251190291987f * dx);
+    put(1.0925484305920792f * dx * dy);
+    put(-1.0925484305920792f * dy * dz);
+    put(0.31539156525252005f * (3.0f * zz - 1.0f));
+    put(-1.0925484305920792f * dx * dz);
+    put(0.5462742152960396f * (xx - yy));
+    put(-0.5900435899266435f * dy * (3.0f * xx - yy));
+    put(2.890611442640554f * dx * dy * dz);
+    put(-0.4570457994644658f * dy * (5.0f * zz - 1.0f));
+    put(0.3731763325901154f * dz * (5.0f * zz - 3.0f));
+    put(-0.4570457994644658f * dx * (5.0f * zz - 1.0f));
+    put(1.445305721320277f * dz * (xx - yy));
+    put(-0.5900435899266435f * dx * (xx - 3.0f * yy));
+    put(q.normal.x); put(q.normal.y); put(q.normal.z);
+    put(q.albedo.x); put(q.albedo.y); put(q.albedo.z);
+    put(q.roughness);
+#pragma unroll
+    for (int i = 0; i < 5; i++) put(0.0f);
 }
 
 struct Scratch {                // per-CTA shared memory header
@@ -191,13 +206,16 @@ __device__ inline void load_weights(unsigned char *w, const unsigned char *g) {
 
 // X (128 x 64, rows = queries) into the core-matrix layout; rows past `count` are zero.
 // `r` is the calling thread's row of the tile.
-__device__ inline void encode_tile(unsigned char *x, const pt_cache_query *q, size_t first, size_t count, const float lo[3],
-                                   const float inv_extent[3], uint32_t r) {
-    float v[64];
+__device__ inline void encode_tile(unsigned char *x, const pt_cache_query *q, size_t first, size_t count, float3 lo,
+                                   float3 inv_extent, uint32_t r) {
     size_t row = first + r;
-    if (row < count) encode(q[row], lo, inv_extent, v);
-    else for (int i = 0; i < 64; i++) v[i] = 0.0f;
-    for (int c = 0; c < 8; c++) store8(x, r, c, 64, v + 8 * c);
+    if (row < count) {
+        RowWriter put{x, r};
+        encode(q[row], lo, inv_extent, put);
+    } else {
+        const float zero[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (int c = 0; c < 8; c++) store8(x, r, c, 64, zero);
+    }
 }
 
 // D[128 x N] (+)= A[128 x K] * B[N x K]^T, A and B K-major in the core layout, K = 16 per MMA.
@@ -249,11 +267,12 @@ struct Sync {
 // activation buffer, one mbarrier and named barrier 1 + g.  One activation buffer suffices: each
 // layer's epilogue runs after that layer's MMA has completed, so it overwrites the MMA's own input.
 // smem: header (Scratch, then the groups' mbarriers from byte 128) | W | pad | (act | pad) x G.
-// Two CTAs of three groups share an SM: six tiles in flight, 2 x 256 TMEM columns.
-constexpr int kFwdGroups = 3;
+// One CTA of eight groups per SM: eight tiles in flight (32 warps at 64 registers), all 512
+// TMEM columns, 188 KB of shared memory.
+constexpr int kFwdGroups = 8;
 constexpr int kFwdThreads = kFwdGroups * kTile;
-constexpr int kFwdCtasPerSm = 2;
-constexpr uint32_t kFwdTmemCols = 256;    // power of two >= 64 * kFwdGroups
+constexpr int kFwdCtasPerSm = 1;
+constexpr uint32_t kFwdTmemCols = 512;    // power of two >= 64 * kFwdGroups
 constexpr size_t kFwdSmem = 256 + kWeightBytes + kPad + kFwdGroups * (kActBytes + kPad);
 static_assert(64 * kFwdGroups <= kFwdTmemCols && kFwdCtasPerSm * kFwdTmemCols <= 512, "TMEM budget");
 static_assert(128 + 8 * kFwdGroups <= 256 && kFwdGroups < 16, "header and named-barrier budget");
@@ -279,8 +298,7 @@ __global__ void __launch_bounds__(kFwdThreads, kFwdCtasPerSm) forward_kernel(con
     const int g = threadIdx.x / kTile;
     const uint32_t r = threadIdx.x % kTile;                        // this thread's row of its group's tile
     unsigned char *act = w + kWeightBytes + kPad + size_t(g) * (kActBytes + kPad);
-    const float l[3] = {lo.x, lo.y, lo.z};
-    const float ie[3] = {1.0f / fmaxf(hi.x - lo.x, 1e-30f), 1.0f / fmaxf(hi.y - lo.y, 1e-30f), 1.0f / fmaxf(hi.z - lo.z, 1e-30f)};
+    const float3 ie = make_float3(1.0f / fmaxf(hi.x - lo.x, 1e-30f), 1.0f / fmaxf(hi.y - lo.y, 1e-30f), 1.0f / fmaxf(hi.z - lo.z, 1e-30f));
     if (threadIdx.x < kFwdGroups) bar_init(&bars[threadIdx.x]);
     tmem_alloc(h, kFwdTmemCols);
     load_weights(w, weights);
@@ -308,10 +326,10 @@ __global__ void __launch_bounds__(kFwdThreads, kFwdCtasPerSm) forward_kernel(con
         fence_after();
         return all;
     };
-    const size_t tiles = (count + kTile - 1) / kTile;
-    const size_t stride = size_t(gridDim.x) * kFwdGroups;
-    for (size_t t = size_t(blockIdx.x) * kFwdGroups + g; t < tiles && ok; t += stride) {
-        encode_tile(act, queries, t * kTile, count, l, ie, r);
+    const uint32_t tiles = uint32_t((count + kTile - 1) / kTile);   // < 2^32: 2^39 queries would not fit in memory
+    const uint32_t stride = gridDim.x * kFwdGroups;
+    for (uint32_t t = blockIdx.x * kFwdGroups + g; t < tiles && ok; t += stride) {
+        encode_tile(act, queries, size_t(t) * kTile, count, lo, ie, r);
         sync_group(true);
         for (int layer = 0; layer < kHidden && ok; layer++) {
             if (issuer) mma_kk(tcol, act, 64, w + layer * kMatBytes, 64, 64, 64, false);
@@ -332,7 +350,7 @@ __global__ void __launch_bounds__(kFwdThreads, kFwdCtasPerSm) forward_kernel(con
         if (done) {
             float v[16];
             tmem_ld16(lane_col, v);
-            size_t row = t * kTile + r;
+            size_t row = size_t(t) * kTile + r;
             if (row < count) { out[3 * row] = expf(v[0]); out[3 * row + 1] = expf(v[1]); out[3 * row + 2] = expf(v[2]); }
         }
         ok = sync_group(done);                    // the next tile's MMAs write these TMEM columns again
@@ -362,8 +380,7 @@ __global__ void __launch_bounds__(kTile, 1) train_kernel(const unsigned char *we
     for (int i = 1; i < 6; i++) act[i] = act[i - 1] + kActBytes + kPad;
     unsigned char *dz = act[5] + kActBytes + kPad;
     unsigned char *dz5 = dz + kActBytes + kPad;
-    const float l[3] = {lo.x, lo.y, lo.z};
-    const float ie[3] = {1.0f / fmaxf(hi.x - lo.x, 1e-30f), 1.0f / fmaxf(hi.y - lo.y, 1e-30f), 1.0f / fmaxf(hi.z - lo.z, 1e-30f)};
+    const float3 ie = make_float3(1.0f / fmaxf(hi.x - lo.x, 1e-30f), 1.0f / fmaxf(hi.y - lo.y, 1e-30f), 1.0f / fmaxf(hi.z - lo.z, 1e-30f));
     if (threadIdx.x == 0) bar_init(&h->bar);
     tmem_alloc(h, 512);
     load_weights(w, weights);
@@ -379,7 +396,7 @@ __global__ void __launch_bounds__(kTile, 1) train_kernel(const unsigned char *we
     const size_t tiles = (count + kTile - 1) / kTile;
     for (size_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
         const size_t row = t * kTile + threadIdx.x;
-        encode_tile(act[0], queries, t * kTile, count, l, ie, threadIdx.x);
+        encode_tile(act[0], queries, t * kTile, count, lo, ie, threadIdx.x);
         fence_async_smem();
         fence_before();
         __syncthreads();
