@@ -39,7 +39,7 @@ struct RenderBuffers {
     int32_t *queue[2];
     int32_t *shadow_queue;
     int32_t *counters;      // [0],[1]: path queues; [2],[3]: shadow queues of even and odd iterations
-    unsigned long long *fetch;   // [0]: extend's item counter, [1],[2]: the shadow kernels' item counters
+    unsigned long long *fetch;   // [0]: extend's item counter, [1],[2]: the shadow kernels' item counters, [3]: finish_pair's
     unsigned long long *rays;
     int32_t *error;
     float *sums;
@@ -64,7 +64,7 @@ __global__ void start_samples(RenderParams p, RenderBuffers b, int32_t count, in
     int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0) {
         b.counters[0] = count; b.counters[1] = 0; b.counters[2] = 0; b.counters[3] = 0;
-        b.fetch[0] = 0; b.fetch[1] = 0; b.fetch[2] = 0;
+        b.fetch[0] = 0; b.fetch[1] = 0; b.fetch[2] = 0; b.fetch[3] = 0;
     }
     if (i >= count) return;
     Pcg rng = b.rng[i];
@@ -208,6 +208,87 @@ __global__ void finish_kernel(DeviceScene scene, RenderParams p, RenderBuffers b
     if ((threadIdx.x & 31) == 0 && rays) atomicAdd(b.rays, rays);
 }
 
+// finish, two lanes per path (four-wide tree, shading views): in each round the even lane of a
+// pair walks the path's next extension ray while the odd lane walks the shadow ray of the path's
+// previous bounce.  A shadow ray only adds to the radiance and the extension ray depends on
+// neither, so a bounce costs one walk's latency instead of two, and both walks run the same
+// instructions (traverse4_rt).  The shadow contribution of bounce k is added before bounce k+1
+// is shaded, as in the one-lane form, so sums, ray counts and streams are bit-identical.  A pair
+// whose path has ended takes the next queue entry from fetch[3] (zeroed before the launch).
+__global__ void __launch_bounds__(256, 2) finish_pair_kernel(DeviceScene scene, RenderParams p, RenderBuffers b, int parity) {
+    const int32_t n = b.counters[parity];
+    const unsigned full = 0xffffffffu;
+    const unsigned lane = threadIdx.x & 31;
+    const bool odd = lane & 1;
+    const unsigned even_lane = lane & ~1u, odd_lane = lane | 1u;
+    unsigned long long rays = 0;
+    int32_t i = -1;                // even lane: the path (slot) in hand, -1 when none
+    PathState s{};
+    Pcg rng{};
+    bool live = false;             // even lane: the path has an extension ray to walk
+    bool pending = false;          // even lane: a shadow ray from the last shading waits
+    bool drained = false;          // even lane: the queue had no entry left for this pair
+    ShadowRay sr{};
+    bool walk_shadow = false;      // odd lane: walks the pair's pending shadow ray this round
+    pt_ray q{};
+    float qmax = 0;
+    for (;;) {
+        if (!odd && !live && !pending && !drained) {
+            if (i >= 0) { b.paths[i] = s; b.rng[i] = rng; i = -1; }
+            unsigned long long k = atomicAdd(&b.fetch[3], 1ull);
+            if (k < (unsigned long long)n) {
+                i = b.queue[parity][k];
+                s = b.paths[i];
+                rng = b.rng[i];
+                live = true;
+            } else {
+                drained = true;
+            }
+        }
+        const bool work = odd ? walk_shadow : live;   // both lanes' rounds stay in step (warp-uniform loop)
+        if (!__any_sync(full, work)) break;
+        HitInfo hi;
+        uint32_t boxes = 0, prims = 0;
+        int error = 0;
+        bool hit = false;
+        if (work) {
+            rays++;   // each query counts once, as trace_color counts it (transport.h:177)
+            hit = traverse4_rt(scene, odd ? q : path_ray(s), 0.001f, odd ? qmax : FLT_MAX, kTieLastLeaf, odd, hi, boxes,
+                               prims, error);
+        }
+        const bool blocked = __shfl_sync(full, hit, odd_lane);
+        const int shadow_error = __shfl_sync(full, error, odd_lane);
+        if (!odd) {
+            if (pending) {
+                if (shadow_error) *b.error = 1;
+                else if (!blocked) { s.rr = s.rr + sr.cr; s.rg = s.rg + sr.cg; s.rb = s.rb + sr.cb; }
+                pending = false;
+            }
+            if (live) {
+                if (error) *b.error = 1;
+                PathHit h;
+                h.t = hi.t; h.u = hi.u; h.v = hi.v; h.slot = (hit && !error) ? hi.slot : (error ? -2 : -1);
+                bool shadow = false;
+                live = shade_path(scene, shade_ctx(p), b.sums + 3 * size_t(i), i, i, s, h, make_uint2(boxes, prims), rng, sr, shadow);
+                pending = shadow;
+            }
+        }
+        // the even lane hands its new shadow ray to the odd lane
+        walk_shadow = __shfl_sync(full, pending, even_lane);
+        q.origin.x = __shfl_sync(full, sr.ox, even_lane);
+        q.origin.y = __shfl_sync(full, sr.oy, even_lane);
+        q.origin.z = __shfl_sync(full, sr.oz, even_lane);
+        q.direction.x = __shfl_sync(full, sr.dx, even_lane);
+        q.direction.y = __shfl_sync(full, sr.dy, even_lane);
+        q.direction.z = __shfl_sync(full, sr.dz, even_lane);
+        q.time = __shfl_sync(full, sr.time, even_lane);
+        qmax = __shfl_sync(full, sr.tmax, even_lane);
+    }
+    if (!odd && i >= 0) { b.paths[i] = s; b.rng[i] = rng; }
+    for (int o = 16; o; o >>= 1) rays += __shfl_down_sync(full, rays, o);
+    if (lane == 0 && rays) atomicAdd(b.rays, rays);
+}
+
 // shadow: any-hit of the NEE rays (transport.h:206-214); unoccluded ones add their contribution
 __global__ void __launch_bounds__(256, 4) shadow_kernel(DeviceScene scene, RenderParams p, RenderBuffers b, int parity, int min_active) {
     const int32_t n = b.counters[2 + parity];
@@ -282,7 +363,7 @@ struct pt_renderer {
     float milliseconds = 0;
     uint64_t rays = 0;
     int block = 256;
-    int grid_extend = 0, grid_shade = 0, grid_shadow = 0, grid_finish = 0;
+    int grid_extend = 0, grid_shade = 0, grid_shadow = 0, grid_finish = 0, grid_finish_pair = 0;
     int32_t tail_paths = 0;             // live-path count below which the fused finish kernel takes over
     DeviceBuffer paths, hits, stats, shadows, queue0, queue1, shadow_queue, counters, fetch, ray_total, error, sums, rng, rgba;
     RenderBuffers buf{};
@@ -302,6 +383,7 @@ struct pt_renderer {
         grid_shade = occupancy_grid((const void *)shade_kernel, block);
         grid_shadow = occupancy_grid((const void *)shadow_kernel, block, stack_bytes(block));
         grid_finish = occupancy_grid((const void *)finish_kernel, block);
+        grid_finish_pair = occupancy_grid((const void *)finish_pair_kernel, block);
     }
 };
 
@@ -350,7 +432,7 @@ pt_status pt_renderer_create(const pt_scene *scene, const pt_camera *camera, int
             r->queue1.resize(n * sizeof(int32_t));
             r->shadow_queue.resize(n * sizeof(int32_t));
             r->counters.resize(4 * sizeof(int32_t));
-            r->fetch.resize(3 * sizeof(unsigned long long));
+            r->fetch.resize(4 * sizeof(unsigned long long));
             r->ray_total.resize(sizeof(unsigned long long));
             r->error.resize(sizeof(int32_t));
             r->sums.resize(n * 3 * sizeof(float));
@@ -367,7 +449,7 @@ pt_status pt_renderer_create(const pt_scene *scene, const pt_camera *camera, int
             PT_CUDA(cudaStreamCreateWithFlags(&r->shadow_stream, cudaStreamNonBlocking));
             PT_CUDA(cudaMallocHost(&r->host_counters, kIterationRing * sizeof(int32_t)));
             r->grids();
-            r->tail_paths = std::max<int32_t>(16384, r->pixels / 8);
+            r->tail_paths = std::max<int32_t>(16384, r->pixels / 4);
         } catch (...) { delete r; throw; }
         *out = r;
         pt_status st = pt_reset(r, camera);
@@ -440,7 +522,12 @@ pt_status pt_add_samples(pt_renderer *r, int count) {
         if (issued > 0) PT_CUDA(cudaStreamWaitEvent(st, r->shadowed[parity ^ 1].get(), 0));
         if (tail && !done) {
             // the few remaining paths (of the last issued iteration's queue) run to completion
-            finish_kernel<<<r->grid_finish, r->block, 0, st>>>(scene, r->params, r->buf, parity);
+            const RenderParams &q = r->params;
+            if (q.wide && !q.brute && q.debug != PT_DEBUG_BVH && q.debug != PT_DEBUG_INTERSECTIONS) {
+                PT_CUDA(cudaMemsetAsync(&r->buf.fetch[3], 0, sizeof(unsigned long long), st));
+                finish_pair_kernel<<<r->grid_finish_pair, r->block, 0, st>>>(scene, q, r->buf, parity);
+            } else
+                finish_kernel<<<r->grid_finish, r->block, 0, st>>>(scene, q, r->buf, parity);
             PT_CUDA(cudaGetLastError());
             done = true;
         }

@@ -66,11 +66,12 @@ PT_HD inline void load_node(const DeviceScene &s, int32_t node, BvhNode &n) {
 #endif
 }
 
-// Tests leaf `slot`; updates the running answer.  Returns true when a hit was accepted.
-template <bool kAny>
-PT_HD inline bool test_leaf(const DeviceScene &s, int32_t slot, const pt_ray &r, float dl, float tmin,
-                            float tmax, int tie, bool &found, float &closest, long long &best_key,
-                            HitInfo &hit, uint32_t &prims) {
+// Tests leaf `slot`; updates the running answer.  Returns true when a hit was accepted.  `any`
+// selects any-hit (the first hit is the answer) or closest-hit (ties by key) at run time; the
+// template below fixes it at compile time.
+PT_HD __forceinline__ bool test_leaf_rt(const DeviceScene &s, int32_t slot, const pt_ray &r, float dl, float tmin,
+                                        float tmax, int tie, bool any, bool &found, float &closest, long long &best_key,
+                                        HitInfo &hit, uint32_t &prims) {
     float limit = found ? nextafterf(closest, tmax) : tmax;
     float t, u = 0, v = 0;
     bool ok;
@@ -85,17 +86,23 @@ PT_HD inline bool test_leaf(const DeviceScene &s, int32_t slot, const pt_ray &r,
         ok = sphere_hit(sp, r, tmin, limit, t);
     }
     if (!ok) return false;
-    if (!kAny && found && !(t < closest)) {
+    if (!any && found && !(t < closest)) {
         long long key = tie_key(s, slot, tie);
         if (!(key < best_key)) return false;
         best_key = key;
-    } else if (!kAny) {
+    } else if (!any) {
         best_key = tie_key(s, slot, tie);
     }
     found = true;
     closest = t;
     hit.t = t; hit.u = u; hit.v = v; hit.slot = slot;
     return true;
+}
+template <bool kAny>
+PT_HD __forceinline__ bool test_leaf(const DeviceScene &s, int32_t slot, const pt_ray &r, float dl, float tmin,
+                                     float tmax, int tie, bool &found, float &closest, long long &best_key,
+                                     HitInfo &hit, uint32_t &prims) {
+    return test_leaf_rt(s, slot, r, dl, tmin, tmax, tie, kAny, found, closest, best_key, hit, prims);
 }
 
 // Closest hit (kAny = false) or any hit (kAny = true) over (tmin, tmax).
@@ -541,21 +548,27 @@ PT_HD inline int node4_children(const DeviceScene &s, int32_t node, const RayBox
     return hits;
 }
 
-// Tests the 1..8 slots of a leaf reference; true when kAny and a hit was found.
-template <bool kAny>
-PT_HD inline bool leaf4(const DeviceScene &s, int32_t ref, const pt_ray &r, float dl, float tmin, float tmax, int tie,
-                        bool &found, float &closest, long long &best_key, HitInfo &hit, uint32_t &prims) {
+// Tests the 1..8 slots of a leaf reference; true when `any` and a hit was found.
+PT_HD __forceinline__ bool leaf4_rt(const DeviceScene &s, int32_t ref, const pt_ray &r, float dl, float tmin, float tmax,
+                                    int tie, bool any, bool &found, float &closest, long long &best_key, HitInfo &hit,
+                                    uint32_t &prims) {
     int32_t v = ~ref;
     int32_t first = v >> 3, count = (v & 7) + 1;
     for (int32_t j = 0; j < count; j++)
-        if (test_leaf<kAny>(s, first + j, r, dl, tmin, tmax, tie, found, closest, best_key, hit, prims) && kAny) return true;
+        if (test_leaf_rt(s, first + j, r, dl, tmin, tmax, tie, any, found, closest, best_key, hit, prims) && any) return true;
     return false;
 }
-
-// Per-thread four-wide walk (local-memory stack), for kernels that run one ray per thread.
 template <bool kAny>
-PT_HD inline bool traverse4(const DeviceScene &s, const pt_ray &r, float tmin, float tmax, int tie,
-                            HitInfo &hit, uint32_t &boxes, uint32_t &prims, int &error, int32_t root = 0) {
+PT_HD __forceinline__ bool leaf4(const DeviceScene &s, int32_t ref, const pt_ray &r, float dl, float tmin, float tmax, int tie,
+                                 bool &found, float &closest, long long &best_key, HitInfo &hit, uint32_t &prims) {
+    return leaf4_rt(s, ref, r, dl, tmin, tmax, tie, kAny, found, closest, best_key, hit, prims);
+}
+
+// Per-thread four-wide walk (local-memory stack), for kernels that run one ray per thread;
+// closest hit or any hit chosen at run time, so that lanes of one warp walking rays of both
+// kinds run the same instructions.
+PT_HD inline bool traverse4_rt(const DeviceScene &s, const pt_ray &r, float tmin, float tmax, int tie, bool any,
+                               HitInfo &hit, uint32_t &boxes, uint32_t &prims, int &error, int32_t root = 0) {
     hit.slot = -1; hit.t = 0; hit.u = 0; hit.v = 0;
     if (s.empty || s.node_count == 0 || root < 0) return false;
     RayBox rb = ray_box(r);
@@ -579,7 +592,7 @@ PT_HD inline bool traverse4(const DeviceScene &s, const pt_ray &r, float tmin, f
                 continue;
             }
         } else {
-            if (leaf4<kAny>(s, cur, r, dl, tmin, tmax, tie, found, closest, best_key, hit, prims) && kAny) return true;
+            if (leaf4_rt(s, cur, r, dl, tmin, tmax, tie, any, found, closest, best_key, hit, prims) && any) return true;
             if (found) limit = nextafterf(closest, tmax);
         }
         // pop the nearest entry still inside the limit
@@ -591,6 +604,11 @@ PT_HD inline bool traverse4(const DeviceScene &s, const pt_ray &r, float tmin, f
         if (!next) break;
     }
     return found;
+}
+template <bool kAny>
+PT_HD inline bool traverse4(const DeviceScene &s, const pt_ray &r, float tmin, float tmax, int tie,
+                            HitInfo &hit, uint32_t &boxes, uint32_t &prims, int &error, int32_t root = 0) {
+    return traverse4_rt(s, r, tmin, tmax, tie, kAny, hit, boxes, prims, error, root);
 }
 
 } // namespace ptb
