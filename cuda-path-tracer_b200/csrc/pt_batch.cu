@@ -51,7 +51,7 @@ struct BatchBuffers {
     int32_t *queue[2];
     int32_t *shadow_queue;
     int32_t *counters;                // [0],[1] path queues, [2],[3] shadow queues of even and odd iterations
-    unsigned long long *fetch;        // [0] extend items, [1],[2] shadow items of even and odd iterations
+    unsigned long long *fetch;        // [0] extend items, [1],[2] shadow items of even and odd iterations, [3] tail slots
     unsigned long long *cursor;       // next pixel to start
     unsigned long long *rays;
     int32_t *job_remaining;
@@ -118,7 +118,7 @@ __global__ void batch_start(BatchBuffers b, int32_t slots) {
     int32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k == 0) {
         b.counters[0] = slots; b.counters[1] = 0; b.counters[2] = 0; b.counters[3] = 0;
-        b.fetch[0] = 0; b.fetch[1] = 0; b.fetch[2] = 0;
+        b.fetch[0] = 0; b.fetch[1] = 0; b.fetch[2] = 0; b.fetch[3] = 0;
         *b.cursor = (unsigned long long)slots;
         *b.start_ns = globaltimer();
         *b.iterations = 0;
@@ -238,57 +238,104 @@ __global__ void batch_control(BatchBuffers b, cudaGraphConditionalHandle handle,
     cudaGraphSetConditional(handle, go ? 1u : 0u);
 }
 
-// The tail: each queued slot runs its paths to the end, taking further pixels while any remain.
-__global__ void batch_finish(DeviceScene scene, BatchBuffers b) {
+// The tail, two lanes per slot: in each round the even lane of a pair walks its path's next ray
+// while the odd lane walks the shadow ray of the path's previous bounce (one runtime-mode walk,
+// traverse4_rt), so a bounce costs one walk's latency instead of two.  The shadow contribution of
+// bounce k is added before bounce k+1 is shaded, the order of the iterations above, so the sums
+// are bit-identical.  A pair whose pixel is done takes the next pixel while any remain, then the next
+// queued slot (fetch[3]).
+__global__ void __launch_bounds__(256, 2) batch_finish_pair(DeviceScene scene, BatchBuffers b) {
     const int32_t n = b.counters[0];
+    const unsigned full = 0xffffffffu;
+    const unsigned lane = threadIdx.x & 31;
+    const bool odd = lane & 1;
+    const unsigned even_lane = lane & ~1u, odd_lane = lane | 1u;
     unsigned long long rays = 0;
-    for (int32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        int32_t slot = b.queue[0][k];
-        PathState s = b.paths[slot];
-        for (;;) {
-            int64_t g = b.slot_pixel[slot];
-            int32_t jid = b.slot_job[slot];
-            const BatchJob &j = b.jobs[jid];
-            DeviceScene js = job_scene(scene, j);
-            Pcg rng = b.rng[g];
-            bool live = true;
-            while (live) {
-                rays++;
-                HitInfo hi;
-                uint32_t boxes = 0, prims = 0;
-                int error = 0;
-                bool hit = traverse4<false>(scene, path_ray(s), 0.001f, FLT_MAX, kTieLastLeaf, hi, boxes, prims, error, j.root);
+    int32_t slot = -1;             // even lane: the slot in hand, -1 when none
+    PathState s{};
+    int64_t g = 0;                 // even lane: the slot's pixel
+    int32_t jid = 0;
+    Pcg rng{};
+    bool live = false;             // even lane: the path has a ray to walk
+    bool pending = false;          // even lane: a shadow ray from the last shading waits
+    bool drained = false;          // even lane: neither pixels nor queued slots are left
+    ShadowRay sr{};
+    bool walk_shadow = false;      // odd lane: walks the pair's pending shadow ray this round
+    pt_ray q{};
+    float qmax = 0;
+    int32_t qroot = 0;
+    for (;;) {
+        if (!odd && !live && !pending && !drained) {
+            if (slot >= 0) {       // the pixel in hand is done
+                b.rng[g] = rng;
+                if (atomicSub(&b.job_remaining[jid], 1) == 1) b.job_done_ns[jid] = globaltimer();
+                unsigned long long next = atomicAdd(b.cursor, 1ull);
+                if (next < (unsigned long long)b.total_pixels) {
+                    start_pixel(b, slot, int64_t(next), s);
+                    g = int64_t(next); jid = b.slot_job[slot]; rng = b.rng[g];
+                    live = true;
+                } else {
+                    b.paths[slot] = s;
+                    slot = -1;
+                }
+            }
+            if (slot < 0) {
+                unsigned long long k = atomicAdd(&b.fetch[3], 1ull);
+                if (k < (unsigned long long)n) {
+                    slot = b.queue[0][k];
+                    s = b.paths[slot]; g = b.slot_pixel[slot]; jid = b.slot_job[slot]; rng = b.rng[g];
+                    live = true;
+                } else {
+                    drained = true;
+                }
+            }
+        }
+        const bool work = odd ? walk_shadow : live;   // both lanes' rounds stay in step (warp-uniform loop)
+        if (!__any_sync(full, work)) break;
+        const int32_t root = odd ? qroot : (live ? b.jobs[jid].root : 0);
+        HitInfo hi;
+        uint32_t boxes = 0, prims = 0;
+        int error = 0;
+        bool hit = false;
+        if (work) {
+            rays++;
+            hit = traverse4_rt(scene, odd ? q : path_ray(s), 0.001f, odd ? qmax : FLT_MAX, kTieLastLeaf, odd, hi, boxes, prims,
+                               error, root);
+        }
+        const bool blocked = __shfl_sync(full, hit, odd_lane);
+        const int shadow_error = __shfl_sync(full, error, odd_lane);
+        if (!odd) {
+            if (pending) {
+                if (shadow_error) *b.error = 1;
+                else if (!blocked) { s.rr = s.rr + sr.cr; s.rg = s.rg + sr.cg; s.rb = s.rb + sr.cb; }
+                pending = false;
+            }
+            if (live) {
                 if (error) *b.error = 1;
+                const BatchJob &j = b.jobs[jid];
+                DeviceScene js = job_scene(scene, j);
                 PathHit h;
                 h.t = hi.t; h.u = hi.u; h.v = hi.v; h.slot = (hit && !error) ? hi.slot : (error ? -2 : -1);
-                ShadowRay sr;
                 bool shadow = false;
                 live = shade_path(js, job_ctx(j, b.mis), b.sums + 3 * g, int32_t(g - j.pixel_offset), slot, s, h, make_uint2(0, 0),
                                   rng, sr, shadow);
-                if (shadow) {
-                    rays++;
-                    pt_ray q;
-                    q.origin = pt_vec3{sr.ox, sr.oy, sr.oz};
-                    q.direction = pt_vec3{sr.dx, sr.dy, sr.dz};
-                    q.time = sr.time;
-                    HitInfo sh;
-                    uint32_t sb = 0, spr = 0;
-                    int serr = 0;
-                    bool blocked = traverse4<true>(scene, q, 0.001f, sr.tmax, kTieLastLeaf, sh, sb, spr, serr, j.root);
-                    if (serr) *b.error = 1;
-                    else if (!blocked) { s.rr = s.rr + sr.cr; s.rg = s.rg + sr.cg; s.rb = s.rb + sr.cb; }
-                }
+                pending = shadow;
             }
-            b.rng[g] = rng;
-            if (atomicSub(&b.job_remaining[jid], 1) == 1) b.job_done_ns[jid] = globaltimer();
-            unsigned long long next = atomicAdd(b.cursor, 1ull);
-            if (next >= (unsigned long long)b.total_pixels) break;
-            start_pixel(b, slot, int64_t(next), s);
         }
-        b.paths[slot] = s;
+        // the even lane hands its new shadow ray (and its job's tree root) to the odd lane
+        walk_shadow = __shfl_sync(full, pending, even_lane);
+        q.origin.x = __shfl_sync(full, sr.ox, even_lane);
+        q.origin.y = __shfl_sync(full, sr.oy, even_lane);
+        q.origin.z = __shfl_sync(full, sr.oz, even_lane);
+        q.direction.x = __shfl_sync(full, sr.dx, even_lane);
+        q.direction.y = __shfl_sync(full, sr.dy, even_lane);
+        q.direction.z = __shfl_sync(full, sr.dz, even_lane);
+        q.time = __shfl_sync(full, sr.time, even_lane);
+        qmax = __shfl_sync(full, sr.tmax, even_lane);
+        qroot = __shfl_sync(full, root, even_lane);
     }
-    for (int o = 16; o; o >>= 1) rays += __shfl_down_sync(0xffffffffu, rays, o);
-    if ((threadIdx.x & 31) == 0 && rays) atomicAdd(b.rays, rays);
+    for (int o = 16; o; o >>= 1) rays += __shfl_down_sync(full, rays, o);
+    if (lane == 0 && rays) atomicAdd(b.rays, rays);
 }
 
 } // namespace ptb
@@ -386,7 +433,7 @@ struct pt_batch {
         batch_control<<<1, 32, 0, stream>>>(buf, handle, tail_paths, max_iterations());
         PT_CUDA(cudaStreamEndCapture(stream, &body));
         PT_CUDA(cudaStreamBeginCaptureToGraph(stream, graph, &loop, nullptr, 1, cudaStreamCaptureModeRelaxed));
-        batch_finish<<<grid((const void *)batch_finish, 0), block, 0, stream>>>(view, buf);
+        batch_finish_pair<<<grid((const void *)batch_finish_pair, 0), block, 0, stream>>>(view, buf);
         PT_CUDA(cudaStreamEndCapture(stream, &graph));
         PT_CUDA(cudaGraphInstantiate(&exec, graph, 0));
     }
@@ -422,7 +469,7 @@ struct pt_batch {
                 if (it + 1 >= bound) { cudaFreeHost(live_host); throw Error(PT_TIMEOUT, "batch did not drain within its iteration bound"); }
             }
             cudaFreeHost(live_host);
-            batch_finish<<<grid((const void *)batch_finish, 0), block, 0, st>>>(view, buf);
+            batch_finish_pair<<<grid((const void *)batch_finish_pair, 0), block, 0, st>>>(view, buf);
         }
         PT_CUDA(cudaGetLastError());
         PT_CUDA(cudaEventRecord(stop.get(), st));
@@ -574,7 +621,7 @@ pt_status pt_batch_create(const pt_scene_desc *scenes, int32_t scene_count, cons
             b->sums.resize(size_t(offset) * 3 * sizeof(float));
             b->rng.resize(size_t(offset) * sizeof(Pcg));
             b->counters.resize(4 * sizeof(int32_t));
-            b->fetch.resize(3 * sizeof(unsigned long long));
+            b->fetch.resize(4 * sizeof(unsigned long long));
             b->scalars.resize(8 * sizeof(unsigned long long));
             b->job_remaining.resize(size_t(job_count) * sizeof(int32_t));
             b->job_done_ns.resize(size_t(job_count) * sizeof(unsigned long long));

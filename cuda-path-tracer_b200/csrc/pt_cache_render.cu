@@ -106,7 +106,7 @@ struct Buffers {
     int32_t *queue[2];
     int32_t *shadow_queue;
     int32_t *counters;                  // [0],[1] path queues, [2] shadow queue, [3] queries, [4] training slots, [5..) batch sizes
-    unsigned long long *fetch;          // item counters of the persistent walks (extend, shadow)
+    unsigned long long *fetch;          // item counters: [0] extend, [1],[2] shadow, [3] finish_pair
     unsigned long long *totals;         // [0] rays, [1] queries, [2] training samples
     int32_t *error;
     float *sums;
@@ -464,6 +464,93 @@ __global__ void finish_kernel(DeviceScene scene, Params p, Buffers b, int parity
     if ((threadIdx.x & 31) == 0 && rays) atomicAdd(&b.totals[0], rays);
 }
 
+// finish, two lanes per path (four-wide tree): in each round the even lane of a pair walks the
+// path's next ray while the odd lane walks the shadow ray of the path's previous bounce, through
+// one runtime-mode walk (traverse4_rt), so a bounce costs one walk's latency instead of two.  A
+// bounce that emits a shadow ray never ends its path sample, and the shadow contribution of
+// bounce k is added before bounce k+1 is shaded (or its sample retired), as in the one-lane
+// form.  A pair whose path has ended takes the next queue entry from fetch[3].
+__global__ void __launch_bounds__(256, 2) finish_pair_kernel(DeviceScene scene, Params p, Buffers b, int parity) {
+    const int32_t n = b.counters[parity];
+    const unsigned full = 0xffffffffu;
+    const unsigned lane = threadIdx.x & 31;
+    const bool odd = lane & 1;
+    const unsigned even_lane = lane & ~1u, odd_lane = lane | 1u;
+    unsigned long long rays = 0;
+    int32_t i = -1;                // even lane: the path (slot) in hand, -1 when none
+    CachePath s{};
+    Pcg rng{};
+    bool live = false;             // even lane: the path has a ray to walk
+    bool pending = false;          // even lane: a shadow ray from the last shading waits
+    bool drained = false;          // even lane: the queue had no entry left for this pair
+    CacheShadow sr{};              // even lane: the pending shadow ray
+    bool walk_shadow = false;      // odd lane: walks the pair's pending shadow ray this round
+    pt_ray q{};
+    float qmax = 0;
+    for (;;) {
+        if (!odd && !live && !pending && !drained) {
+            if (i >= 0) { b.paths[i] = s; b.rng[i] = rng; i = -1; }
+            unsigned long long k = atomicAdd(&b.fetch[3], 1ull);
+            if (k < (unsigned long long)n) {
+                i = b.queue[parity][k];
+                s = b.paths[i];
+                rng = b.rng[i];
+                live = true;
+            } else {
+                drained = true;
+            }
+        }
+        const bool work = odd ? walk_shadow : live;   // both lanes' rounds stay in step (warp-uniform loop)
+        if (!__any_sync(full, work)) break;
+        HitInfo hi;
+        uint32_t boxes = 0, prims = 0;
+        int error = 0;
+        bool hit = false;
+        if (work) {
+            rays++;
+            hit = traverse4_rt(scene, odd ? q : cache_ray(s), 0.001f, odd ? qmax : FLT_MAX, kTieLastLeaf, odd, hi, boxes, prims,
+                               error);
+        }
+        const bool blocked = __shfl_sync(full, hit, odd_lane);
+        const int shadow_error = __shfl_sync(full, error, odd_lane);
+        if (!odd) {
+            if (pending) {
+                if (shadow_error) *b.error = 1;
+                else if (!blocked) {
+                    s.rr += sr.cr; s.rg += sr.cg; s.rb += sr.cb;
+                    if (sr.suffix) { s.sr += sr.sr; s.sg += sr.sg; s.sb += sr.sb; }
+                }
+                pending = false;
+            }
+            if (live) {
+                if (error) *b.error = 1;
+                PathHit h;
+                h.t = hi.t; h.u = hi.u; h.v = hi.v; h.slot = (hit && !error) ? hi.slot : (error ? -2 : -1);
+                ShadeOut o;
+                shade(scene, p, b, i, s, h, rng, o);
+                if (o.shadow) { sr = o.sr; pending = true; }
+                if (o.finished) {
+                    const int32_t qi = o.query ? atomicAdd(&b.counters[3], 1) : -1;
+                    live = retire(p, b, i, s, rng, o, qi);
+                }
+            }
+        }
+        // the even lane hands its new shadow ray to the odd lane
+        walk_shadow = __shfl_sync(full, pending, even_lane);
+        q.origin.x = __shfl_sync(full, sr.ox, even_lane);
+        q.origin.y = __shfl_sync(full, sr.oy, even_lane);
+        q.origin.z = __shfl_sync(full, sr.oz, even_lane);
+        q.direction.x = __shfl_sync(full, sr.dx, even_lane);
+        q.direction.y = __shfl_sync(full, sr.dy, even_lane);
+        q.direction.z = __shfl_sync(full, sr.dz, even_lane);
+        q.time = __shfl_sync(full, sr.time, even_lane);
+        qmax = __shfl_sync(full, sr.tmax, even_lane);
+    }
+    if (!odd && i >= 0) { b.paths[i] = s; b.rng[i] = rng; }
+    for (int o = 16; o; o >>= 1) rays += __shfl_down_sync(full, rays, o);
+    if (lane == 0 && rays) atomicAdd(&b.totals[0], rays);
+}
+
 __global__ void __launch_bounds__(256, 4) shadow_kernel(DeviceScene scene, Params p, Buffers b, int parity, int min_active) {
     const int32_t n = b.counters[kShadowSlot + parity];
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&b.totals[0], (unsigned long long)n);
@@ -575,7 +662,7 @@ struct pt_cached_renderer {
     int frames = 0;
     float milliseconds = 0;
     int block = 256;
-    int grid_extend = 0, grid_shade = 0, grid_shadow = 0, grid_finish = 0, grid_small = 0;
+    int grid_extend = 0, grid_shade = 0, grid_shadow = 0, grid_finish = 0, grid_finish_pair = 0, grid_small = 0;
     DeviceBuffer paths, hits, shadows, queue0, queue1, shadow_queue, counters, fetch, totals, error, sums, rng, frame;
     DeviceBuffer queries, aux, pred, pixel_queries, pixel_query_count, vertices, ends, samples, targets;
     Buffers buf{};
@@ -610,7 +697,7 @@ struct pt_cached_renderer {
     }
     void prologue(const Params &p, cudaStream_t st) {
         PT_CUDA(cudaMemsetAsync(buf.counters, 0, kCounters * sizeof(int32_t), st));
-        PT_CUDA(cudaMemsetAsync(buf.fetch, 0, 3 * sizeof(unsigned long long), st));
+        PT_CUDA(cudaMemsetAsync(buf.fetch, 0, 4 * sizeof(unsigned long long), st));
         PT_CUDA(cudaMemsetAsync(buf.pairs, 0, sizeof(unsigned long long), st));
         start_kernel<<<(pixels + 255) / 256, 256, 0, st>>>(p, buf, pixels);
         PT_CUDA(cudaGetLastError());
@@ -634,7 +721,8 @@ struct pt_cached_renderer {
     }
     // the fused kernel ends the paths left in queue 0, then the network's part of the frame
     void epilogue(const Params &p, cudaStream_t st) {
-        finish_kernel<<<grid_finish, block, 0, st>>>(scene->view, p, buf, 0);
+        if (p.wide) finish_pair_kernel<<<grid_finish_pair, block, 0, st>>>(scene->view, p, buf, 0);
+        else finish_kernel<<<grid_finish, block, 0, st>>>(scene->view, p, buf, 0);
         PT_CUDA(cudaGetLastError());
         if (p.use_cache) {
             cache_forward(cache, buf.queries, query_capacity(), &buf.counters[3], buf.pred, st);
@@ -809,7 +897,7 @@ pt_status pt_cached_create(const pt_scene *scene, const pt_camera *camera, int w
             r->queue1.resize(n * sizeof(int32_t));
             r->shadow_queue.resize(n * sizeof(int32_t));
             r->counters.resize(kCounters * sizeof(int32_t));
-            r->fetch.resize(3 * sizeof(unsigned long long));
+            r->fetch.resize(4 * sizeof(unsigned long long));
             r->totals.resize(3 * sizeof(unsigned long long));
             r->error.resize(sizeof(int32_t));
             r->sums.resize(n * 3 * sizeof(float));
@@ -852,6 +940,7 @@ pt_status pt_cached_create(const pt_scene *scene, const pt_camera *camera, int w
             r->grid_shade = occupancy_grid((const void *)shade_kernel, r->block, 0);
             r->grid_shadow = occupancy_grid((const void *)shadow_kernel, r->block, stack_bytes(r->block));
             r->grid_finish = occupancy_grid((const void *)finish_kernel, r->block, 0);
+            r->grid_finish_pair = occupancy_grid((const void *)finish_pair_kernel, r->block, 0);
             r->grid_small = device_sm_count() * 4;
             // pixel RNG streams as the plain renderer seeds them (pixel_rng.seed(seed, pixel))
             std::vector<Pcg> streams(n);
