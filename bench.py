@@ -522,13 +522,12 @@ def run_render(args):
                     "images_bit_identical": bool(same), "speedup": value / (rrays / rms / 1e3)}
     cpu = None
     if REF_CPU_SO.exists():
-        small, small_cam = pt.procedural_scene(240, 150)
         threads = os.cpu_count() or 1
         t = time.perf_counter()
-        _, _, crays = RefCpu().render(small, small_cam, 240, 150, 1, [4], nthreads=threads)
+        _, _, crays = RefCpu().render(scene, cam, W, H, 1, [16], nthreads=threads)
         dt = time.perf_counter() - t
         cpu = {"value": crays / dt / 1e6, "unit": "Mrays/s", "cores": threads, "kind": "reference",
-               "sample": f"reference trace_pixel_sample (bounce limit 50) on 240x150 x 4 spp: {crays} rays in {dt:.2f} s"}
+               "sample": f"reference trace_pixel_sample (bounce limit 50) on the same scene, {W}x{H} x 16 spp: {crays} rays in {dt:.2f} s"}
     line = {"metric": "Mrays/s render (procedural 1M, 960x600, 64 spp, depth 8, MIS)", "value": value, "unit": "Mrays/s",
             "n_gpus": 1, "steps": steps, "warmup": max(1, args.warmup), "ms_per_step": ms / steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",

@@ -935,7 +935,7 @@ pt_status pt_cached_create(const pt_scene *scene, const pt_camera *camera, int w
             PT_CUDA(cudaMallocHost(&r->live_host, sizeof(int32_t)));
             r->pairs.resize(sizeof(unsigned long long));
             b.pairs = r->pairs.get<unsigned long long>();
-            r->tail_paths = cfg.tail_paths > 0 ? cfg.tail_paths : std::max<int32_t>(16384, int32_t(n / 32));
+            r->tail_paths = cfg.tail_paths > 0 ? cfg.tail_paths : std::max<int32_t>(16384, int32_t(n / 16));
             r->grid_extend = occupancy_grid((const void *)extend_kernel, r->block, stack_bytes(r->block));
             r->grid_shade = occupancy_grid((const void *)shade_kernel, r->block, 0);
             r->grid_shadow = occupancy_grid((const void *)shadow_kernel, r->block, stack_bytes(r->block));

@@ -300,7 +300,7 @@ typedef struct pt_cached_params {
     float learning_rate;        /* Adam learning rate (1e-2; beta 0.9 / 0.99) */
     uint64_t network_seed;      /* weight initialisation */
     int32_t tail_paths;         /* live paths below which one fused kernel ends the frame's tail
-                                 * (0: max(16384, pixels / 32)) */
+                                 * (0: max(16384, pixels / 16)) */
     int32_t query_specular;     /* 1 (default): paths may also end at metal and glass vertices;
                                  * 0: at diffuse vertices only */
     float weight_average;       /* decay of the weight average queries use (0.99; 0: the live weights) */
