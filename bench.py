@@ -524,10 +524,10 @@ def run_render(args):
     if REF_CPU_SO.exists():
         threads = os.cpu_count() or 1
         t = time.perf_counter()
-        _, _, crays = RefCpu().render(scene, cam, W, H, 1, [16], nthreads=threads)
+        _, _, crays = RefCpu().render(scene, cam, W, H, 1, [SPP], nthreads=threads)
         dt = time.perf_counter() - t
         cpu = {"value": crays / dt / 1e6, "unit": "Mrays/s", "cores": threads, "kind": "reference",
-               "sample": f"reference trace_pixel_sample (bounce limit 50) on the same scene, {W}x{H} x 16 spp: {crays} rays in {dt:.2f} s"}
+               "sample": f"reference trace_pixel_sample (bounce limit 50) on the same scene, {W}x{H} x {SPP} spp: {crays} rays in {dt:.2f} s"}
     line = {"metric": "Mrays/s render (procedural 1M, 960x600, 64 spp, depth 8, MIS)", "value": value, "unit": "Mrays/s",
             "n_gpus": 1, "steps": steps, "warmup": max(1, args.warmup), "ms_per_step": ms / steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
