@@ -697,7 +697,10 @@ def main():
                    "parallelism": f"replicas x{world}"},
         "kernel_ms": kernel_ms, "kernel_stats_per_ray": {"child_boxes": stats[0], "primitives": stats[1]},
         "hit_rate": hit_rate, "scene_build_s": t_scene, "bvh": args.bvh, "gpu_bvh_build_s": t_gpu_build,
-        "clocks": clock, "gpu_launches": args.steps,
+        "clocks": clock,
+        # per step: the ray-key kernel, the radix sort of the keys (CUB DeviceRadixSort, 30 bits)
+        # and the walk kernel; the sort's own kernels are counted as one launch here
+        "gpu_launches": 3 * args.steps,
         "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
     }
     if rank == 0:

@@ -60,7 +60,7 @@ void require_device();
 int device_sm_count();
 
 // Tunables of the traversal kernels (pt_query_tuning; the autotuner sets them).
-struct QueryConfig { int persistent = 1; int min_active = 16; int blocks_per_sm = 0; int wide = 1; int speculative = 1; };
+struct QueryConfig { int persistent = 1; int min_active = 16; int blocks_per_sm = 0; int wide = 1; int speculative = 1; int order = 1; };
 extern QueryConfig g_query_config;
 
 } // namespace ptb
@@ -78,6 +78,7 @@ struct pt_scene {
     cudaStream_t streams[3] = {nullptr, nullptr, nullptr};
     ptb::DeviceBuffer ray_counter;          // per-launch ray counters of the persistent query kernel
     unsigned counter_slot = 0;
+    cudaMemPool_t order_pool = nullptr;     // stream-ordered scratch of the ray ordering (kept, not released)
     int device = 0;
     ~pt_scene();
 };

@@ -2,6 +2,7 @@
 //
 // Replaces cuda_query_rays / query_rays (src/cuda/cuda_renderer.cu:111-120, 248-260) and the
 // device_scene upload (src/cuda/cuda_renderer.cu:36-54).
+#include <cub/device/device_radix_sort.cuh>
 #include <cfloat>
 #include <algorithm>
 #include <cstring>
@@ -55,18 +56,25 @@ __global__ void __launch_bounds__(kQueryBlock) query_kernel(DeviceScene s, const
 // Persistent form: a fixed grid of warps; each warp takes rays from a global counter and,
 // between traversal steps, hands a new ray to every lane whose ray has ended once fewer than
 // `min_active` lanes are still busy.  next_ray must be zero at launch.
+// `order` (may be null) lists the rays in the order they are taken: the k-th ray taken is
+// rays[order[k]], and its answer goes to hits[order[k]].
 template <bool kAny, bool kStats, int kWalk>
 __global__ void __launch_bounds__(kQueryBlock) query_persistent_kernel(DeviceScene s, const pt_ray *__restrict__ rays, size_t count,
                                                                        float tmin, const float *__restrict__ tmax,
                                                                        pt_hit *__restrict__ hits, pt_ray_stats *__restrict__ stats,
-                                                                       int tie, unsigned long long *next_ray, int min_active) {
-    auto get = [&](size_t k, pt_ray &r, float &lo, float &hi) { r = rays[k]; lo = tmin; hi = tmax ? tmax[k] : FLT_MAX; };
+                                                                       int tie, unsigned long long *next_ray, int min_active,
+                                                                       const uint32_t *__restrict__ order) {
+    auto get = [&](size_t k, pt_ray &r, float &lo, float &hi) {
+        const size_t i = order ? size_t(order[k]) : k;
+        r = rays[i]; lo = tmin; hi = tmax ? tmax[i] : FLT_MAX;
+    };
     auto done = [&](size_t k, const WalkResult &w) {
+        const size_t i = order ? size_t(order[k]) : k;
         bool hit = w.slot >= 0;
         int32_t type = PT_BRANCH, id = -1;
         if (hit) hit_ids(s, w.slot, type, id);
-        reinterpret_cast<int4 *>(hits)[k] = make_int4(__float_as_int(hit ? w.t : 0.0f), id, type, w.error);
-        if (kStats) { stats[k].boxes = w.boxes; stats[k].primitives = w.prims; }
+        reinterpret_cast<int4 *>(hits)[i] = make_int4(__float_as_int(hit ? w.t : 0.0f), id, type, w.error);
+        if (kStats) { stats[i].boxes = w.boxes; stats[i].primitives = w.prims; }
     };
     if (kWalk == 2) persistent_walk4_spec<kAny>(s, count, next_ray, min_active, tie, get, done);
     else if (kWalk == 1) persistent_walk4<kAny>(s, count, next_ray, min_active, tie, get, done);
@@ -141,6 +149,65 @@ __global__ void bounce_rays_kernel(DeviceScene s, const pt_ray *primary, const p
 
 unsigned grid_for(size_t count, int block) { return unsigned((count + size_t(block) - 1) / size_t(block)); }
 
+// ---- ray ordering -----------------------------------------------------------------------------
+// A batch of at least kOrderMin rays is walked in the order of a 30-bit key: the direction's
+// octant (3 bits) above a Morton code of the origin in the scene's root box (9 bits per axis).
+// Rays that start close together and head the same way then share warps and walk the same nodes:
+// fewer idle lanes, more cache hits.  The sort is stable and only changes which lane walks which
+// ray, so every answer is the same.
+constexpr size_t kOrderMin = size_t(1) << 18;
+constexpr int kOrderBits = 30;
+
+__device__ inline uint32_t spread_bits3(uint32_t v) {   // 9 bits -> every third bit of 27
+    v &= 0x1ffu;
+    v = (v | (v << 16)) & 0x030000ffu;
+    v = (v | (v << 8)) & 0x0300f00fu;
+    v = (v | (v << 4)) & 0x030c30c3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+
+__global__ void ray_keys_kernel(const pt_ray *__restrict__ rays, size_t count, float3 lo, float3 scale, uint32_t *__restrict__ keys,
+                                uint32_t *__restrict__ index) {
+    size_t k = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    const pt_ray r = rays[k];
+    // fmaxf(NaN, 0) is 0: a non-finite origin still gets a key
+    uint32_t x = uint32_t(fminf(fmaxf((r.origin.x - lo.x) * scale.x, 0.0f), 511.0f));
+    uint32_t y = uint32_t(fminf(fmaxf((r.origin.y - lo.y) * scale.y, 0.0f), 511.0f));
+    uint32_t z = uint32_t(fminf(fmaxf((r.origin.z - lo.z) * scale.z, 0.0f), 511.0f));
+    uint32_t octant = (r.direction.x < 0.0f ? 1u : 0u) | (r.direction.y < 0.0f ? 2u : 0u) | (r.direction.z < 0.0f ? 4u : 0u);
+    keys[k] = (octant << 27) | spread_bits3(x) | (spread_bits3(y) << 1) | (spread_bits3(z) << 2);
+    index[k] = uint32_t(k);
+}
+
+// Sorts the batch's ray indices by key into scratch from the scene's memory pool (allocated and
+// freed in stream order, so concurrent queries on other streams get their own).  Returns the
+// order and the scratch to free after the walk.
+const uint32_t *order_rays(const pt_scene *sc, const pt_ray *rays, size_t count, cudaStream_t stream, void *&scratch) {
+    const DeviceScene &s = sc->view;
+    float3 lo = make_float3(s.root_lo[0], s.root_lo[1], s.root_lo[2]);
+    float3 scale;
+    float ext[3] = {s.root_hi[0] - s.root_lo[0], s.root_hi[1] - s.root_lo[1], s.root_hi[2] - s.root_lo[2]};
+    scale.x = ext[0] > 0 ? 512.0f / ext[0] : 0.0f;
+    scale.y = ext[1] > 0 ? 512.0f / ext[1] : 0.0f;
+    scale.z = ext[2] > 0 ? 512.0f / ext[2] : 0.0f;
+    const int n = int(count);
+    size_t temp = 0;
+    PT_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, temp, (const uint32_t *)nullptr, (uint32_t *)nullptr,
+                                            (const uint32_t *)nullptr, (uint32_t *)nullptr, n, 0, kOrderBits, stream));
+    const size_t words = (count + 63) & ~size_t(63);          // 256-byte aligned sub-arrays
+    const size_t bytes = 4 * words * sizeof(uint32_t) + temp;
+    PT_CUDA(cudaMallocFromPoolAsync(&scratch, bytes, sc->order_pool, stream));
+    uint32_t *keys_in = static_cast<uint32_t *>(scratch), *keys_out = keys_in + words;
+    uint32_t *index_in = keys_out + words, *index_out = index_in + words;
+    void *temp_storage = index_out + words;
+    ray_keys_kernel<<<grid_for(count, 256), 256, 0, stream>>>(rays, count, lo, scale, keys_in, index_in);
+    PT_CUDA(cudaGetLastError());
+    PT_CUDA(cub::DeviceRadixSort::SortPairs(temp_storage, temp, keys_in, keys_out, index_in, index_out, n, 0, kOrderBits, stream));
+    return index_out;
+}
+
 // Query kernel variant and its tunables (the autotuner sets these).
 QueryConfig g_query_config;
 
@@ -156,7 +223,7 @@ void launch_query(const pt_scene *sc, const pt_ray *rays, size_t count, int mode
         const bool wide = g_query_config.wide && s.nodes4;
         const bool any = mode == PT_QUERY_ANY;
         using Fn = void (*)(DeviceScene, const pt_ray *, size_t, float, const float *, pt_hit *, pt_ray_stats *, int,
-                            unsigned long long *, int);
+                            unsigned long long *, int, const uint32_t *);
         static const Fn table[12] = {
             query_persistent_kernel<false, false, 0>, query_persistent_kernel<false, false, 1>, query_persistent_kernel<false, false, 2>,
             query_persistent_kernel<false, true, 0>, query_persistent_kernel<false, true, 1>, query_persistent_kernel<false, true, 2>,
@@ -171,8 +238,17 @@ void launch_query(const pt_scene *sc, const pt_ray *rays, size_t count, int mode
         int bps = g_query_config.blocks_per_sm > 0 ? std::min(g_query_config.blocks_per_sm, per_sm[k]) : per_sm[k];
         size_t want = (count + kQueryBlock - 1) / kQueryBlock;
         unsigned grid = unsigned(std::min<size_t>(want, size_t(device_sm_count()) * size_t(bps > 0 ? bps : 1)));
-        fn<<<grid, kQueryBlock, smem, stream>>>(s, rays, count, tmin, tmax, hits, stats, tie, counter, g_query_config.min_active);
+        void *scratch = nullptr;
+        const uint32_t *order = nullptr;
+        if (g_query_config.order && count >= kOrderMin && count <= size_t(INT32_MAX) && sc->order_pool) {
+            cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+            PT_CUDA(cudaStreamIsCapturing(stream, &capture));
+            if (capture == cudaStreamCaptureStatusNone) order = order_rays(sc, rays, count, stream, scratch);   // not inside a graph capture
+        }
+        fn<<<grid, kQueryBlock, smem, stream>>>(s, rays, count, tmin, tmax, hits, stats, tie, counter, g_query_config.min_active,
+                                                 order);
         PT_CUDA(cudaGetLastError());
+        if (scratch) PT_CUDA(cudaFreeAsync(scratch, stream));
         return;
     }
     unsigned grid = grid_for(count, kQueryBlock);
@@ -190,6 +266,7 @@ void launch_query(const pt_scene *sc, const pt_ray *rays, size_t count, int mode
 
 pt_scene::~pt_scene() {
     for(auto &s : streams) if(s) cudaStreamDestroy(s);
+    if(order_pool) { cudaDeviceSynchronize(); cudaMemPoolDestroy(order_pool); }
 }
 
 extern "C" {
@@ -232,6 +309,15 @@ pt_status pt_scene_create(const pt_scene_desc *desc, pt_scene **out) {
         auto sc = new pt_scene;
         try {
             PT_CUDA(cudaGetDevice(&sc->device));
+            {   // the ray ordering's scratch pool: memory stays with the pool between queries
+                cudaMemPoolProps props{};
+                props.allocType = cudaMemAllocationTypePinned;
+                props.location.type = cudaMemLocationTypeDevice;
+                props.location.id = sc->device;
+                PT_CUDA(cudaMemPoolCreate(&sc->order_pool, &props));
+                uint64_t keep = UINT64_MAX;
+                PT_CUDA(cudaMemPoolSetAttribute(sc->order_pool, cudaMemPoolAttrReleaseThreshold, &keep));
+            }
             sc->host_lights = lights;
             sc->light_area = area;
             sc->triangle_count = desc->triangle_count;
@@ -391,6 +477,11 @@ pt_status pt_query_walk(int speculative) {
     return guard([&]() { g_query_config.speculative = speculative ? 1 : 0; });
 }
 
+// Ray ordering of large batches: 1 = walk rays in (octant, origin Morton code) order, 0 = as given.
+pt_status pt_query_order(int enabled) {
+    return guard([&]() { g_query_config.order = enabled ? 1 : 0; });
+}
+
 // ---- no-allocation query ---------------------------------------------------------------------
 // Scratch of pt_query_rays_static, shared by every call on a device: the persistent kernel's
 // ray counter, then staging for PT_STATIC_QUERY_MAX_RAYS rays, tmax values, hits and counters.
@@ -451,7 +542,7 @@ pt_status pt_query_rays_static(const pt_scene *scene, const pt_ray *rays, size_t
         const bool wide = s.nodes4 != nullptr;
         const bool any = mode == PT_QUERY_ANY;
         using Fn = void (*)(DeviceScene, const pt_ray *, size_t, float, const float *, pt_hit *, pt_ray_stats *, int,
-                            unsigned long long *, int);
+                            unsigned long long *, int, const uint32_t *);
         static const Fn table[8] = {
             query_persistent_kernel<false, false, 0>, query_persistent_kernel<false, false, 2>,
             query_persistent_kernel<false, true, 0>, query_persistent_kernel<false, true, 2>,
@@ -463,7 +554,7 @@ pt_status pt_query_rays_static(const pt_scene *scene, const pt_ray *rays, size_t
         PT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)fn, kQueryBlock, smem));
         size_t want = (count + kQueryBlock - 1) / kQueryBlock;
         unsigned grid = unsigned(std::min<size_t>(want, size_t(device_sm_count()) * size_t(per_sm > 0 ? per_sm : 1)));
-        fn<<<grid, kQueryBlock, smem, st>>>(s, d_rays, count, tmin, d_tmax, d_hits, d_stats, kTieLowestId, counter, 16);
+        fn<<<grid, kQueryBlock, smem, st>>>(s, d_rays, count, tmin, d_tmax, d_hits, d_stats, kTieLowestId, counter, 16, nullptr);
         PT_CUDA(cudaGetLastError());
         PT_CUDA(cudaMemcpyAsync(hits, d_hits, count * sizeof(pt_hit), cudaMemcpyDeviceToHost, st));
         if(stats) PT_CUDA(cudaMemcpyAsync(stats, d_stats, count * sizeof(pt_ray_stats), cudaMemcpyDeviceToHost, st));

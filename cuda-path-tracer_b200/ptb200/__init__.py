@@ -118,6 +118,7 @@ def library() -> C.CDLL:
         "pt_query_tuning": (I, [I, I, I]),
         "pt_query_layout": (I, [I]),
         "pt_query_walk": (I, [I]),
+        "pt_query_order": (I, [I]),
         "pt_rays_camera_device": (I, [P, I, I, U64, U64, S, P, P]),
         "pt_rays_bounce_device": (I, [P, P, P, S, U64, U64, P, P]),
         "pt_flat_from_desc": (I, [P, P]),
@@ -452,6 +453,11 @@ def query_layout(wide: int = 1) -> None:
 def query_walk(speculative: int = 1) -> None:
     """Four-wide walk form: node/leaf phases (1) or a single loop (0) (pt_query_walk)."""
     check(library().pt_query_walk(int(speculative)))
+
+
+def query_order(enabled: int = 1) -> None:
+    """Ray ordering of large batches by (octant, origin Morton code) (pt_query_order)."""
+    check(library().pt_query_order(int(enabled)))
 
 
 def cuda_query_rays(scene: FlatScene, rays: np.ndarray, brute: bool = False) -> np.ndarray:

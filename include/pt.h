@@ -172,6 +172,11 @@ pt_status pt_query_layout(int wide);
 /* Four-wide walk form (process-wide): 1 = separate node and leaf phases per warp round, lanes
  * that already hold a leaf walking on speculatively (default); 0 = nodes and leaves in one loop. */
 pt_status pt_query_walk(int speculative);
+/* Ray ordering (process-wide): 1 = batches of at least 2^18 rays are walked in the order of a key
+ * made of the direction's octant and a Morton code of the origin (a stable sort; lanes of a warp
+ * then walk neighbouring rays), answers written back in the caller's order (default); 0 = rays are
+ * taken as given.  Results do not depend on it.  pt_query_rays_static never reorders. */
+pt_status pt_query_order(int enabled);
 
 /* ---- device ray generators (bit-identical to the host ones in pt_workloads.h) ----
  * Camera rays of pt_rays_camera; bounce rays from closest hits: origin at the hit, a

@@ -190,6 +190,44 @@ def test_procedural_scene_vs_oracle(oracle, layout):
     assert np.array_equal(got["primitive_type"] != 0, want["primitive_id"] >= 0)
 
 
+def test_ray_order_keeps_answers(oracle, layout):
+    """Batches of at least 2^18 rays are walked in (octant, origin Morton code) order: the hits
+    and any-hit answers are the same bytes as walking the rays as given, and a sample of them
+    equals the oracle's.  (The per-ray walk counters are not compared: in the phased walk a lane
+    holding a leaf walks on while its warp finishes the node phase, so its counts depend on which
+    rays share the warp.)"""
+    torch = pytest.importorskip("torch")
+    s, cam = pt.procedural_scene(160, 100, sphere_count=5, segments=96, rings=49, seed=8, random_triangles=5000)
+    dev = pt.Scene(s)
+    n = 1 << 18
+    rays = torch.zeros(2 * n * 28, dtype=torch.uint8, device="cuda")
+    hits = torch.zeros(n * 16, dtype=torch.uint8, device="cuda")
+    pt.camera_rays_device(cam, 160, 100, 1, 0, n, rays)
+    dev.query_device(rays, n, hits)
+    dev.bounce_rays_device(rays, hits, n, 2, 0, rays[n * 28:])
+    tmax = torch.rand(2 * n, generator=torch.Generator(device="cuda").manual_seed(3), device="cuda") * 20
+    out = {}
+    try:
+        for order in (0, 1):
+            pt.query_order(order)
+            h = torch.zeros(2 * n * 16, dtype=torch.uint8, device="cuda")
+            st = torch.zeros(2 * n * 8, dtype=torch.uint8, device="cuda")
+            a = torch.zeros(2 * n * 16, dtype=torch.uint8, device="cuda")
+            dev.query_device(rays, 2 * n, h, stats=st)
+            dev.query_device(rays, 2 * n, a, mode=pt.QUERY_ANY, tmax=tmax)
+            torch.cuda.synchronize()
+            out[order] = (h.cpu().numpy(), a.cpu().numpy())
+    finally:
+        pt.query_order(1)
+    for x, y in zip(out[0], out[1]):
+        assert x.tobytes() == y.tobytes()
+    got = out[1][0].view(pt.HIT)
+    assert (got["primitive_type"] != 0).mean() > 0.3
+    host = rays.cpu().numpy().view(pt.RAY)
+    pick = np.r_[0:2048, n:n + 2048]
+    assert_hits_equal(got[pick], oracle.query(s, host[pick]))
+
+
 @pytest.mark.skipif(not REF_GPU_SO.exists(), reason="reference CUDA build absent")
 def test_matches_reference_gpu_query(layout):
     """Our compatibility query and the reference's own cuda_query_rays on the same B200."""
