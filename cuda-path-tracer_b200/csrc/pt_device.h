@@ -60,7 +60,7 @@ void require_device();
 int device_sm_count();
 
 // Tunables of the traversal kernels (pt_query_tuning; the autotuner sets them).
-struct QueryConfig { int persistent = 1; int min_active = 16; int blocks_per_sm = 0; int wide = 1; int speculative = 1; int order = 1; };
+struct QueryConfig { int persistent = 1; int min_active = 8; int blocks_per_sm = 0; int wide = 1; int speculative = 1; int order = 1; };
 extern QueryConfig g_query_config;
 
 } // namespace ptb

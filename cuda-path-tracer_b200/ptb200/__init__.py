@@ -440,7 +440,7 @@ def camera_rays_device(camera: np.ndarray, width, height, seed, first, count, ou
     check(library().pt_rays_camera_device(camera.ctypes.data, width, height, seed, first, count, _ptr(out), stream))
 
 
-def query_tuning(persistent: int = 1, min_active: int = 16, blocks_per_sm: int = 0) -> None:
+def query_tuning(persistent: int = 1, min_active: int = 8, blocks_per_sm: int = 0) -> None:
     """Sets the ray-query kernel variant and its tunables (pt_query_tuning)."""
     check(library().pt_query_tuning(persistent, min_active, blocks_per_sm))
 

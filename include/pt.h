@@ -163,7 +163,7 @@ pt_status pt_query_rays_brute_device(const pt_scene *scene, const pt_ray *rays, 
 /* Tuning of the ray-query kernel (process-wide): persistent = 1 runs a fixed grid of warps that
  * take rays from a global counter and refill lanes whose ray has ended once fewer than
  * `min_active` (1..32) lanes are busy; persistent = 0 launches one thread per ray.
- * blocks_per_sm = 0 uses the occupancy limit.  Defaults: 1, 16, 0. */
+ * blocks_per_sm = 0 uses the occupancy limit.  Defaults: 1, 8, 0. */
 pt_status pt_query_tuning(int persistent, int min_active, int blocks_per_sm);
 /* Node layout of the traversal kernels (process-wide; renderers pick it up when created):
  * 1 = four-wide nodes (up to 4 primitives per leaf) where the scene's tree allows it (default),
