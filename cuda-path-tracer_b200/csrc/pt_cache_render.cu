@@ -412,8 +412,9 @@ __global__ void shade_kernel(DeviceScene scene, Params p, Buffers b, int parity)
 }
 
 // finish: the queue's remaining paths run to their end, one thread per path (extend, shade and
-// shadow fused).  Runs after the first few wavefront iterations, where the queue is short and a
-// wavefront iteration would cost the latency of its slowest ray for a handful of rays.
+// shadow fused).  Runs once the queue is short, where a wavefront iteration would cost the
+// latency of its slowest ray for a handful of rays; used on two-wide trees (four-wide trees take
+// finish_pair_kernel below).
 __global__ void finish_kernel(DeviceScene scene, Params p, Buffers b, int parity) {
     const int32_t n = b.counters[parity];
     unsigned long long rays = 0;

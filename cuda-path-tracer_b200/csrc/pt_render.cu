@@ -157,7 +157,8 @@ __global__ void __launch_bounds__(256, 4) shade_kernel(DeviceScene scene, Render
 
 // finish: the queue's remaining paths run to the end of their pixel's samples, one thread per
 // path (the reference's megakernel form).  Used once the queue is short, where a wavefront
-// iteration would cost the latency of its slowest ray for a handful of rays.
+// iteration would cost the latency of its slowest ray for a handful of rays, on two-wide trees,
+// with the brute-force walk and for the bvh / intersections views (otherwise finish_pair_kernel).
 __global__ void finish_kernel(DeviceScene scene, RenderParams p, RenderBuffers b, int parity) {
     const int32_t n = b.counters[parity];
     const bool reference_order = p.debug == PT_DEBUG_BVH || p.debug == PT_DEBUG_INTERSECTIONS;
