@@ -177,6 +177,49 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+class Ranks:
+    """One process per GPU, launched by torchrun: rank, world size, a barrier and the maximum over
+    ranks of a measured time.  The closest-hit workload shards as independent replicas (each rank
+    walks its own batch; nothing is exchanged on the data path), so the only collectives are the
+    barrier around the timed region and the max of the ranks' times.  backend "nccl" keeps the
+    reduction on the GPU; "gloo" on the host serves the multi-process tests."""
+
+    def __init__(self, backend: str = "nccl", timeout_s: int = 300):
+        import torch
+        import torch.distributed as dist
+        self.dist = dist
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.device = torch.device("cuda", self.local) if backend == "nccl" else torch.device("cpu")
+        if self.world > 1 and not dist.is_initialized():
+            from datetime import timedelta
+            extra = {"device_id": self.device} if backend == "nccl" else {}
+            dist.init_process_group(backend, timeout=timedelta(seconds=timeout_s), **extra)
+
+    def barrier(self) -> None:
+        if self.world > 1:
+            self.dist.barrier()
+
+    def max(self, x: float) -> float:
+        if self.world == 1:
+            return x
+        import torch
+        t = torch.tensor([x], device=self.device, dtype=torch.float64)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self) -> None:
+        if self.world > 1 and self.dist.is_initialized():
+            self.dist.destroy_process_group()
+
+
+def whole_job_rate(world: int, units_per_rank: int, steps: int, max_seconds: float) -> float:
+    """Units all ranks processed per second of the slowest rank (weak scaling: every rank does
+    units_per_rank per step)."""
+    return world * units_per_rank * steps / max_seconds
+
+
 def batch_jobs(count: int, gpu_bvh: bool = False):
     """Seeded render jobs 1..count: log-uniform 10k-2M triangles and 256x256-1920x1080 pixels,
     8-64 spp, bounce limit 4-12, scenes in the style of the procedural 1M-triangle scene."""
@@ -558,26 +601,11 @@ def main():
         run_render(args)
         return
     import torch
-    import torch.distributed as dist
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    if world > 1:
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    ranks = Ranks("nccl")
+    world, rank, local = ranks.world, ranks.rank, ranks.local
+    barrier, max_over_ranks = ranks.barrier, ranks.max
 
     scene, cam, t_scene = build_scene()
     t_gpu_build = None
@@ -618,7 +646,7 @@ def main():
     total_ms = max_over_ranks(start.elapsed_time(stop))
     per_launch_ms = [a.elapsed_time(b) for a, b in ev]
     kernel_ms = float(np.mean(per_launch_ms))
-    value = world * n * args.steps / (total_ms / 1e3) / 1e9
+    value = whole_job_rate(world, n, args.steps, total_ms / 1e3) / 1e9
 
     # kernel-own traversal counters (one untimed launch)
     st = torch.empty(n * 8, dtype=torch.uint8, device="cuda")
@@ -649,7 +677,7 @@ def main():
             e2e_step()
         torch.cuda.synchronize()
         e_dt = max_over_ranks(time.perf_counter() - t)
-        e2e = {"value": world * n * e_steps / e_dt / 1e9, "unit": UNIT, "h2d_bytes_per_step": n * 28,
+        e2e = {"value": whole_job_rate(world, n, e_steps, e_dt) / 1e9, "unit": UNIT, "h2d_bytes_per_step": n * 28,
                "d2h_bytes_per_step": n * 16, "ms_per_step": e_dt / e_steps * 1e3,
                "api": "pt_query_rays (host buffers, 3-stream chunked pipeline)"}
         assert h_hits.numpy().view(pt.HIT).size == len(r_np)
@@ -706,8 +734,7 @@ def main():
     if rank == 0:
         print(json.dumps(line), flush=True)
     del dev
-    if world > 1:
-        dist.destroy_process_group()
+    ranks.close()
 
 
 if __name__ == "__main__":
