@@ -1,19 +1,19 @@
 // pt_jpeg.cpp — baseline (sequential, 8-bit, Huffman) JPEG decoding into 8-bit RGB for OBJ
-// textures, with the sample arithmetic of the loader the reference's image_texture uses
-// (third_party/stb_image.h of the reference, requested with 3 channels), so that decoded texels
-// are the same bytes:
+// textures (ITU-T T.81), with the sample arithmetic of the loader the reference's image_texture
+// uses (its third_party image loader, requested with 3 channels), so that decoded texels are the
+// same bytes.  The arithmetic is fixed by that bar; the code is this library's own:
 //   * coefficients dequantised while decoding and kept as int16;
-//   * the integer inverse DCT of the IJG "islow" method (Loeffler–Ligtenberg–Moschytz, constants
-//     in 12-bit fixed point), columns first with 2 extra bits kept (rounding 512 >> 10), rows
-//     with rounding 2^16 and the +128 level shift before >> 17, clamped to 0..255; a column whose
-//     AC terms are all zero takes 4 * DC;
-//   * chroma upsampled to the full grid with the centred triangle filters (3:1 weights;
-//     2x2: (3 * (3 n + f) + (3 n' + f') + 8) >> 4 inside a row, (3 n + f + 2) >> 2 at its ends;
+//   * the inverse DCT is the islow integer method (Loeffler-Ligtenberg-Moschytz constants in
+//     12-bit fixed point), evaluated as two passes of an integer basis-matrix product (columns
+//     kept with 2 extra bits, rounding 2^9 >> 10; rows with rounding 2^16 and the +128 level
+//     shift before >> 17; clamped to 0..255) — the same integers the factorised flow produces;
+//   * chroma upsampled to the full grid with centred triangle filters (3:1 weights; 2x2:
+//     (3 v + v' + 8) >> 4 over the vertical blend v = 3 near + far, clamped at the row ends;
 //     2x1 and 1x2 likewise), other ratios by replication;
-//   * YCbCr to RGB in fixed point: y << 20 plus 2^19, Cr * 1.402, Cr * -0.71414 plus the Cb term
-//     * -0.34414 truncated to its upper 16 bits, Cb * 1.772, each constant rounded to 12 bits and
-//     shifted by 8, result >> 20 clamped; three components stored as R, G, B directly when they
-//     are labelled 'R' 'G' 'B' or an Adobe marker says so in a file without JFIF;
+//   * YCbCr to RGB in 20-bit fixed point from per-chroma lookup tables (1.402, -0.71414 and
+//     -0.34414 with its product truncated to the upper 16 bits, 1.772), result >> 20 clamped;
+//     three components stored as R, G, B directly when they are labelled 'R' 'G' 'B' or an
+//     Adobe marker says so in a file without JFIF;
 //   * one component: grey replicated.
 // Progressive, lossless, arithmetic-coded, 12-bit and four-component files are rejected.
 #include <algorithm>
@@ -99,119 +99,120 @@ struct Bits {
 
 inline uint8_t clamp8(int x) { return (unsigned)x > 255 ? (x < 0 ? 0 : 255) : uint8_t(x); }
 
-// 12-bit fixed-point constants of the islow inverse DCT
-constexpr int fix(float x) { return int(double(x * 4096) + 0.5); }
+// 12-bit fixed point, rounded as (int)(x * 4096 + 0.5) of the signed value (so a negative
+// constant rounds toward zero after the + 0.5).
+constexpr int q12(float x) { return int(double(x * 4096) + 0.5); }
 
-// one 8-point inverse DCT pass; s[] are the inputs at stride `stride`, results in out[8]
-// before the caller's rounding/shift (even part x0..x3, odd part t0..t3 as in the islow method)
-inline void idct_1d(const int *s, int stride, int &x0, int &x1, int &x2, int &x3, int &t0, int &t1, int &t2, int &t3) {
-    int p2 = s[2 * stride], p3 = s[6 * stride];
-    int p1 = (p2 + p3) * fix(0.5411961f);
-    t2 = p1 + p3 * fix(-1.847759065f);
-    t3 = p1 + p2 * fix(0.765366865f);
-    p2 = s[0];
-    p3 = s[4 * stride];
-    t0 = (p2 + p3) * 4096;
-    t1 = (p2 - p3) * 4096;
-    x0 = t0 + t3; x3 = t0 - t3; x1 = t1 + t2; x2 = t1 - t2;
-    t0 = s[7 * stride]; t1 = s[5 * stride]; t2 = s[3 * stride]; t3 = s[1 * stride];
-    p3 = t0 + t2;
-    int p4 = t1 + t3;
-    p1 = t0 + t3;
-    p2 = t1 + t2;
-    int p5 = (p3 + p4) * fix(1.175875602f);
-    t0 = t0 * fix(0.298631336f);
-    t1 = t1 * fix(2.053119869f);
-    t2 = t2 * fix(3.072711026f);
-    t3 = t3 * fix(1.501321110f);
-    p1 = p5 + p1 * fix(-0.899976223f);
-    p2 = p5 + p2 * fix(-2.562915447f);
-    p3 = p3 * fix(-1.961570560f);
-    p4 = p4 * fix(-0.390180644f);
-    t3 += p1 + p4;
-    t2 += p2 + p3;
-    t1 += p2 + p4;
-    t0 += p1 + p3;
-}
-
-void idct_block(uint8_t *out, int stride, const int16_t coef[64]) {
-    int tmp[64], in[64];
-    for (int i = 0; i < 64; i++) in[i] = coef[i];
-    for (int c = 0; c < 8; c++) {
-        const int *d = in + c;
-        if (!d[8] && !d[16] && !d[24] && !d[32] && !d[40] && !d[48] && !d[56]) {
-            int dc = d[0] * 4;
-            for (int r = 0; r < 8; r++) tmp[c + 8 * r] = dc;
-            continue;
+// Inverse-DCT basis: kBasis.m[n][k] multiplies frequency k in sample n.  The islow method
+// evaluates the Loeffler-Ligtenberg-Moschytz factorisation: shared butterflies with 12 rounded
+// rotation constants.  Every step of it is an exact integer addition or multiplication, so each
+// sample of a 1-D pass equals the dot product of the frequencies with one row of an integer
+// matrix, whose entry is the sum of the rounded constants on the flow graph's paths from that
+// frequency to that sample; this table holds those sums.
+struct IdctBasis { int m[8][8]; };
+constexpr IdctBasis make_idct_basis() {
+    IdctBasis b{};
+    const int r0541 = q12(0.5411961f), r0765 = q12(0.765366865f), n1847 = q12(-1.847759065f);
+    const int r1175 = q12(1.175875602f), r0298 = q12(0.298631336f), r2053 = q12(2.053119869f);
+    const int r3072 = q12(3.072711026f), r1501 = q12(1.501321110f), n0899 = q12(-0.899976223f);
+    const int n2562 = q12(-2.562915447f), n1961 = q12(-1.961570560f), n0390 = q12(-0.390180644f);
+    // even frequencies 0, 2, 4, 6: four sums, sample m and sample 7 - m both add sum m
+    const int even[4][4] = {{4096, r0541 + r0765, 4096, r0541},
+                            {4096, r0541, -4096, r0541 + n1847},
+                            {4096, -r0541, -4096, -(r0541 + n1847)},
+                            {4096, -(r0541 + r0765), 4096, -r0541}};
+    // odd frequencies 1, 3, 5, 7: four sums, sample m adds sum m and sample 7 - m subtracts it;
+    // each carries r1175 (f1 + f3 + f5 + f7) and the rotations of its own paths
+    const int odd[4][4] = {{r1175 + r1501 + n0899 + n0390, r1175, r1175 + n0390, r1175 + n0899},
+                           {r1175, r1175 + r3072 + n2562 + n1961, r1175 + n2562, r1175 + n1961},
+                           {r1175 + n0390, r1175 + n2562, r1175 + r2053 + n2562 + n0390, r1175},
+                           {r1175 + n0899, r1175 + n1961, r1175, r1175 + r0298 + n0899 + n1961}};
+    for (int m = 0; m < 4; m++) {
+        for (int j = 0; j < 4; j++) {
+            b.m[m][2 * j] = even[m][j];
+            b.m[7 - m][2 * j] = even[m][j];
+            b.m[m][2 * j + 1] = odd[m][j];
+            b.m[7 - m][2 * j + 1] = -odd[m][j];
         }
-        int x0, x1, x2, x3, t0, t1, t2, t3;
-        idct_1d(d, 8, x0, x1, x2, x3, t0, t1, t2, t3);
-        x0 += 512; x1 += 512; x2 += 512; x3 += 512;
-        tmp[c + 0] = (x0 + t3) >> 10; tmp[c + 56] = (x0 - t3) >> 10;
-        tmp[c + 8] = (x1 + t2) >> 10; tmp[c + 48] = (x1 - t2) >> 10;
-        tmp[c + 16] = (x2 + t1) >> 10; tmp[c + 40] = (x2 - t1) >> 10;
-        tmp[c + 24] = (x3 + t0) >> 10; tmp[c + 32] = (x3 - t0) >> 10;
     }
+    return b;
+}
+constexpr IdctBasis kIdct = make_idct_basis();
+
+// 8x8 inverse DCT of dequantised coefficients (natural order) into 8-bit samples: a pass over the
+// columns kept with 2 extra bits (x 2^-10, rounded), a pass over the rows (x 2^-17, rounded, with
+// the +128 level shift), clamped to 0..255.  Sums wrap modulo 2^32 as 32-bit integer code does.
+void idct8x8(uint8_t *out, int stride, const int16_t coef[64]) {
+    int mid[64];
+    for (int c = 0; c < 8; c++) {
+        for (int n = 0; n < 8; n++) {
+            int64_t acc = 512;
+            for (int k = 0; k < 8; k++) acc += int64_t(kIdct.m[n][k]) * coef[8 * k + c];
+            mid[8 * n + c] = int32_t(uint32_t(acc)) >> 10;
+        }
+    }
+    const int64_t bias = 65536 + (int64_t(128) << 17);
     for (int r = 0; r < 8; r++) {
-        int x0, x1, x2, x3, t0, t1, t2, t3;
-        idct_1d(tmp + 8 * r, 1, x0, x1, x2, x3, t0, t1, t2, t3);
-        const int bias = 65536 + (128 << 17);
-        x0 += bias; x1 += bias; x2 += bias; x3 += bias;
-        uint8_t *o = out + r * stride;
-        o[0] = clamp8((x0 + t3) >> 17); o[7] = clamp8((x0 - t3) >> 17);
-        o[1] = clamp8((x1 + t2) >> 17); o[6] = clamp8((x1 - t2) >> 17);
-        o[2] = clamp8((x2 + t1) >> 17); o[5] = clamp8((x2 - t1) >> 17);
-        o[3] = clamp8((x3 + t0) >> 17); o[4] = clamp8((x3 - t0) >> 17);
+        for (int n = 0; n < 8; n++) {
+            int64_t acc = bias;
+            for (int k = 0; k < 8; k++) acc += int64_t(kIdct.m[n][k]) * mid[8 * r + k];
+            out[r * stride + n] = clamp8(int32_t(uint32_t(acc)) >> 17);
+        }
     }
 }
 
-// One full-resolution row of a component from its stored rows `near` and `far` (w samples).
+// One full-resolution row of a component from its stored rows `near` (nearest to the output
+// row) and `far` (the one beyond it), w stored samples, hs x vs subsampling.  Triangle filters:
+// vertically 3 near + far; horizontally every output sample weighs its own stored sample 3:1
+// against the neighbour on its side, the neighbour clamped to the row.  For 2x1 the loader the
+// reference uses computes the second-to-last sample of a row (w >= 2) from the last two stored
+// samples weighted 3:1 toward the earlier one; that is kept.
 void upsample_row(uint8_t *out, const uint8_t *near, const uint8_t *far, int w, int hs, int vs) {
     if (hs == 1 && vs == 1) { std::memcpy(out, near, size_t(w)); return; }
     if (hs == 1 && vs == 2) { for (int i = 0; i < w; i++) out[i] = uint8_t((3 * near[i] + far[i] + 2) >> 2); return; }
-    if (hs == 2 && vs == 1) {
-        if (w == 1) { out[0] = out[1] = near[0]; return; }
-        out[0] = near[0];
-        out[1] = uint8_t((near[0] * 3 + near[1] + 2) >> 2);
-        int i;
-        for (i = 1; i < w - 1; i++) {
-            int n = 3 * near[i] + 2;
-            out[2 * i] = uint8_t((n + near[i - 1]) >> 2);
-            out[2 * i + 1] = uint8_t((n + near[i + 1]) >> 2);
+    if (hs == 2 && (vs == 1 || vs == 2)) {
+        // v[i]: the vertical blend in quarter units (vs == 2) or the stored sample (vs == 1)
+        auto v = [&](int i) { return vs == 2 ? 3 * near[i] + far[i] : int(near[i]); };
+        const int shift = vs == 2 ? 4 : 2, round = 1 << (shift - 1);
+        int prev = v(0), cur = prev;
+        for (int i = 0; i < w; i++) {
+            int next = i + 1 < w ? v(i + 1) : cur;
+            out[2 * i] = uint8_t((3 * cur + prev + round) >> shift);
+            out[2 * i + 1] = uint8_t((3 * cur + next + round) >> shift);
+            prev = cur;
+            cur = next;
         }
-        out[2 * i] = uint8_t((near[w - 2] * 3 + near[w - 1] + 2) >> 2);
-        out[2 * i + 1] = near[w - 1];
-        return;
-    }
-    if (hs == 2 && vs == 2) {
-        if (w == 1) { out[0] = out[1] = uint8_t((3 * near[0] + far[0] + 2) >> 2); return; }
-        int t1 = 3 * near[0] + far[0];
-        out[0] = uint8_t((t1 + 2) >> 2);
-        for (int i = 1; i < w; i++) {
-            int t0 = t1;
-            t1 = 3 * near[i] + far[i];
-            out[2 * i - 1] = uint8_t((3 * t0 + t1 + 8) >> 4);
-            out[2 * i] = uint8_t((3 * t1 + t0 + 8) >> 4);
-        }
-        out[2 * w - 1] = uint8_t((t1 + 2) >> 2);
+        if (vs == 1 && w >= 2) out[2 * w - 2] = uint8_t((3 * near[w - 2] + near[w - 1] + 2) >> 2);
         return;
     }
     for (int i = 0; i < w; i++)
         for (int j = 0; j < hs; j++) out[i * hs + j] = near[i];
 }
 
-constexpr int cfix(float x) { return int(x * 4096.0f + 0.5f) << 8; }
+// YCbCr to RGB in 20-bit fixed point with the JFIF matrix (1.402, -0.71414, -0.34414, 1.772,
+// each rounded to 12 bits then scaled by 2^8), the products looked up per chroma value; the Cb
+// term of green keeps only its upper 16 bits, as the reference's loader computes it.
+struct ChromaTables { int cr_r[256], cr_g[256], cb_g[256], cb_b[256]; };
+constexpr int q20(float x) { return int(x * 4096.0f + 0.5f) << 8; }
+constexpr ChromaTables make_chroma_tables() {
+    ChromaTables t{};
+    for (int value = 0; value < 256; value++) {
+        const int c = value - 128;
+        t.cr_r[value] = c * q20(1.40200f);
+        t.cr_g[value] = c * -q20(0.71414f);
+        t.cb_g[value] = int(unsigned(c * -q20(0.34414f)) & 0xffff0000u);
+        t.cb_b[value] = c * q20(1.77200f);
+    }
+    return t;
+}
+constexpr ChromaTables kChroma = make_chroma_tables();
 
-void ycbcr_row(uint8_t *out, const uint8_t *y, const uint8_t *cb, const uint8_t *cr, int count) {
+void ycbcr_to_rgb(uint8_t *rgb, const uint8_t *y, const uint8_t *cb, const uint8_t *cr, int count) {
     for (int i = 0; i < count; i++) {
-        int yf = (y[i] << 20) + (1 << 19);
-        int r_ = cr[i] - 128, b_ = cb[i] - 128;
-        int r = yf + r_ * cfix(1.40200f);
-        int g = yf + (r_ * -cfix(0.71414f)) + int(unsigned(b_ * -cfix(0.34414f)) & 0xffff0000u);
-        int b = yf + b_ * cfix(1.77200f);
-        out[3 * i] = clamp8(r >> 20);
-        out[3 * i + 1] = clamp8(g >> 20);
-        out[3 * i + 2] = clamp8(b >> 20);
+        const int base = (int(y[i]) << 20) | (1 << 19);
+        rgb[3 * i + 0] = clamp8((base + kChroma.cr_r[cr[i]]) >> 20);
+        rgb[3 * i + 1] = clamp8((base + kChroma.cr_g[cr[i]] + kChroma.cb_g[cb[i]]) >> 20);
+        rgb[3 * i + 2] = clamp8((base + kChroma.cb_b[cb[i]]) >> 20);
     }
 }
 
@@ -349,7 +350,7 @@ bool decode_jpeg(const std::vector<unsigned char> &file, Image &img, std::string
                     k++;
                     coef[zig] = int16_t(bits.receive_extend(s) * quant[c.tq][zig]);
                 }
-                idct_block(&c.plane[size_t(by) * 8 * size_t(c.w2) + size_t(bx) * 8], c.w2, coef);
+                idct8x8(&c.plane[size_t(by) * 8 * size_t(c.w2) + size_t(bx) * 8], c.w2, coef);
                 return true;
             };
             int todo = restart_interval ? restart_interval : 0x7fffffff;
@@ -425,7 +426,7 @@ bool decode_jpeg(const std::vector<unsigned char> &file, Image &img, std::string
         uint8_t *out = &img.rgb[size_t(y) * size_t(width) * 3];
         if (n == 3) {
             if (is_rgb) for (int i = 0; i < width; i++) { out[3 * i] = row[0][i]; out[3 * i + 1] = row[1][i]; out[3 * i + 2] = row[2][i]; }
-            else ycbcr_row(out, row[0], row[1], row[2], width);
+            else ycbcr_to_rgb(out, row[0], row[1], row[2], width);
         } else {
             for (int i = 0; i < width; i++) out[3 * i] = out[3 * i + 1] = out[3 * i + 2] = row[0][i];
         }
