@@ -340,6 +340,17 @@ __global__ void __launch_bounds__(256, 2) batch_finish_pair(DeviceScene scene, B
 
 } // namespace ptb
 
+namespace ptb {
+// Four pinned host words for the host-driven loop's read-backs, freed on every path out.
+struct PinnedWords {
+    int32_t *words = nullptr;
+    PinnedWords() { PT_CUDA(cudaMallocHost(&words, 4 * sizeof(int32_t))); }
+    ~PinnedWords() { if (words) cudaFreeHost(words); }
+    PinnedWords(const PinnedWords &) = delete;
+    PinnedWords &operator=(const PinnedWords &) = delete;
+};
+} // namespace ptb
+
 struct pt_batch {
     DeviceScene view{};
     DeviceBuffer nodes4, tris, spheres, triangles, sphere_src, materials, textures, pixels, lights, jobs;
@@ -351,6 +362,7 @@ struct pt_batch {
     int mis = 1;
     // tuning (pt_batch_tuning / pt_batch_autotune)
     int32_t capacity = 0, block = 256, min_active = 16, tail_paths = 16384, use_graph = 1;
+    int32_t probe_fault_countdown = 0;   // > 0: that autotune probe run fails on the host (tests)
     int32_t slots = 0;
     BatchBuffers buf{};
     cudaStream_t stream = nullptr;
@@ -456,19 +468,17 @@ struct pt_batch {
         } else {
             // host-driven form of the same loop: iterations in pairs, live count read back each pair
             unsigned long long bound = max_iterations();
-            int32_t *live_host = nullptr;
-            PT_CUDA(cudaMallocHost(&live_host, 2 * sizeof(int64_t)));
+            PinnedWords live_host;
             unsigned long long cursor = 0;
             for (unsigned long long it = 0;; it++) {
                 pair(st);
-                PT_CUDA(cudaMemcpyAsync(live_host, buf.counters, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+                PT_CUDA(cudaMemcpyAsync(live_host.words, buf.counters, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
                 PT_CUDA(cudaMemcpyAsync(&cursor, buf.cursor, sizeof cursor, cudaMemcpyDeviceToHost, st));
                 PT_CUDA(cudaStreamSynchronize(st));
-                int32_t live = live_host[0];
+                int32_t live = live_host.words[0];
                 if (live == 0 || (live < tail_paths && cursor >= (unsigned long long)total_pixels)) break;
-                if (it + 1 >= bound) { cudaFreeHost(live_host); throw Error(PT_TIMEOUT, "batch did not drain within its iteration bound"); }
+                if (it + 1 >= bound) throw Error(PT_TIMEOUT, "batch did not drain within its iteration bound");
             }
-            cudaFreeHost(live_host);
             batch_finish_pair<<<grid((const void *)batch_finish_pair, 0), block, 0, st>>>(view, buf);
         }
         PT_CUDA(cudaGetLastError());
@@ -683,6 +693,15 @@ pt_status pt_batch_stats(const pt_batch *b, float *kernel_ms, uint64_t *rays, do
     });
 }
 
+// Fault injection for tests, on the host: the n-th autotune probe run from now fails as a timed-out
+// run would (n <= 0: none).
+pt_status pt_batch_fail_probe(pt_batch *b, int32_t n) {
+    return guard([&]() {
+        if (!b) throw Error(PT_INVALID_ARGUMENT, "null batch");
+        b->probe_fault_countdown = n > 0 ? n : 0;
+    });
+}
+
 // Autotuner: times probe runs (every job at min(probe_samples, its samples)) over path-pool
 // capacity, block size, refill threshold and graph/host loop, keeps the fastest, and caches it per
 // (log2 triangles, log2 pixels) bucket in a text file (one "bucket capacity block min_active
@@ -708,22 +727,37 @@ pt_status pt_batch_autotune(pt_batch *b, int32_t probe_samples, const char *cach
             }
         }
         if (!cached) {
-            // probe: fewer samples per job
-            std::vector<BatchJob> saved = b->host_jobs;
+            // probe: fewer samples per job; the jobs' own sample counts come back on every path out
+            struct Restore {
+                pt_batch *b;
+                std::vector<BatchJob> saved;
+                ~Restore() {
+                    b->host_jobs = saved;
+                    try { b->jobs.upload(b->host_jobs); } catch (...) {}
+                }
+            } restore{b, b->host_jobs};
             for (auto &j : b->host_jobs) j.samples = std::min(j.samples, probe_samples);
             b->jobs.upload(b->host_jobs);
             const int32_t caps[] = {1 << 20, 1 << 21, 1 << 22};
             const int32_t blocks[] = {128, 256};
             const int32_t actives[] = {8, 16, 24};
             double best_ms = 1e30;
+            std::string failure;
             for (int32_t cap : caps) for (int32_t blk : blocks) for (int32_t act : actives) for (int32_t graph : {1, 0}) {
                 pt_status st = pt_batch_tuning(b, cap, blk, act, b->tail_paths, graph);
                 if (st != PT_OK) continue;
-                b->run();
+                try {
+                    if (b->probe_fault_countdown > 0 && --b->probe_fault_countdown == 0)
+                        throw Error(PT_TIMEOUT, "probe run failed (injected on the host)");
+                    b->run();
+                } catch (const Error &e) {
+                    if (e.status == PT_CUDA_ERROR) throw;   // the context may be lost: stop the sweep
+                    failure = e.what();                      // this setting failed: skip it
+                    continue;
+                }
                 if (b->milliseconds < best_ms) { best_ms = b->milliseconds; cfg[0] = cap; cfg[1] = blk; cfg[2] = act; cfg[3] = graph; }
             }
-            b->host_jobs = saved;
-            b->jobs.upload(b->host_jobs);
+            if (best_ms == 1e30) throw Error(PT_INVALID_ARGUMENT, "every autotune setting failed: " + failure);
             if (cache_path) {
                 std::ofstream outf(cache_path, std::ios::app);
                 outf << bucket << " " << cfg[0] << " " << cfg[1] << " " << cfg[2] << " " << cfg[3] << " " << best_ms << "\n";

@@ -2,6 +2,8 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <atomic>
+#include <mutex>
 #include <string>
 #include <vector>
 #include "pt_host.h"
@@ -58,6 +60,9 @@ private:
 
 void require_device();
 int device_sm_count();
+// Ray counters per scene: launches further apart than this many may share one counter, so a scene
+// takes at most this many persistent-kernel launches in flight at once.
+constexpr int kRayCounters = 64;
 
 // Tunables of the traversal kernels (pt_query_tuning; the autotuner sets them).
 struct QueryConfig { int persistent = 1; int min_active = 8; int blocks_per_sm = 0; int wide = 1; int speculative = 1; int order = 1; };
@@ -76,9 +81,13 @@ struct pt_scene {
     // host-buffer query workspace (reused between calls)
     ptb::DeviceBuffer work_rays[3], work_tmax[3], work_hits[3], work_stats[3];
     cudaStream_t streams[3] = {nullptr, nullptr, nullptr};
-    ptb::DeviceBuffer ray_counter;          // per-launch ray counters of the persistent query kernel
-    unsigned counter_slot = 0;
+    std::mutex work_mutex;                  // one pt_query_rays call at a time uses the workspace above
+    ptb::DeviceBuffer ray_counter;          // per-launch ray counters of the persistent query kernel (a ring)
+    std::atomic<unsigned> counter_slot{0};
     cudaMemPool_t order_pool = nullptr;     // stream-ordered scratch of the ray ordering (kept, not released)
     int device = 0;
+    // pt_query_profile: CUDA events recorded around each walk-kernel launch (pairs, a ring)
+    std::vector<cudaEvent_t> profile_events;
+    size_t profile_next = 0;
     ~pt_scene();
 };

@@ -184,6 +184,27 @@ PT_HD inline void surface_point(const pt_triangle *tris, uint64_t count, Pcg &r,
     if (r.uniform() < 0.5f) n = -n;
 }
 
+// One surface ray (pt_rays_surface / pt_rays_surface_device): origin a random surface point;
+// with `shadow`, aimed at a second surface point with *tmax = distance - 0.001 (the shadow query
+// of src/renderer/transport.h:206-208), else a cosine-distributed direction about the normal.
+PT_HD inline void surface_ray(const pt_triangle *tris, uint64_t count, uint64_t seed, uint64_t index, bool shadow,
+                              pt_ray &out, float *tmax) {
+    Pcg r; r.seed(seed, index);
+    f3 p, n;
+    surface_point(tris, count, r, p, n);
+    out.origin = pv(p); out.time = 0;
+    if (shadow) {
+        f3 q, m;
+        surface_point(tris, count, r, q, m);
+        f3 d = q - p;
+        float dist = length(d);
+        out.direction = pv(dist > 0 ? d / dist : n);
+        *tmax = dist > 0.002f ? dist - 0.001f : 0.001f;
+    } else {
+        out.direction = pv(cosine_lift(n, r));
+    }
+}
+
 // One bounce ray (pt_rays_bounce / pt_rays_bounce_device): shared by host and device.
 PT_HD inline void bounce_ray(const pt_triangle *tris, uint64_t tri_count, const pt_sphere *spheres, const pt_ray &r,
                              const pt_hit &h, uint64_t seed, uint64_t index, pt_ray &out) {

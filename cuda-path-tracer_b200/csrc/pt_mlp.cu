@@ -12,8 +12,10 @@
 // (LBO = 128 B between K core matrices, SBO = C*16 B between row groups); read transposed it is
 // the canonical MN-major layout (SBO = 128 B, LBO = C*16 B).  So activations, gradients and
 // weights are each stored once and used both ways: X*W, dZ*W^T and X^T*dZ.
-// Every mbarrier wait is bounded: on expiry the kernel records PT_TIMEOUT in its status word,
-// stops issuing, frees its TMEM and returns.
+// Every mbarrier wait is bounded: on expiry the kernel records PT_TIMEOUT in its status word and
+// stops issuing; a group whose wait ran out then waits once more, with the full limit, for the
+// MMAs it had committed (so no MMA still writes TMEM), frees its TMEM and returns.  The reduce and
+// Adam kernels leave the weights alone while the status word is set.
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -38,7 +40,7 @@ constexpr int kActBytes = kTile * kWidth * 2;              // 16 KB per 128 x 64
 constexpr int kOutActBytes = kTile * kOutPad * 2;          // 4 KB per 128 x 16 tile
 constexpr int kPad = 2048;                                 // guard after every operand buffer
 constexpr int kMasterFloats = kHidden * kWidth * kWidth + kWidth * kOut;   // 20672
-constexpr long long kSpinLimit = 1ll << 22;
+constexpr long long kSpinLimit = 1ll << 22;   // mbarrier try_wait attempts before a wait gives up
 
 // byte offset of element (r, c) of a matrix with `cols` columns in the core-matrix layout
 __host__ __device__ inline uint32_t canon(uint32_t r, uint32_t c, uint32_t cols) {
@@ -79,10 +81,10 @@ __device__ inline void bar_init(uint64_t *bar) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(bar)) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
-// bounded wait for the phase with parity `phase` to complete
-__device__ inline bool bar_wait(uint64_t *bar, uint32_t phase) {
+// bounded wait for the phase with parity `phase` to complete: at most `attempts` try_waits
+__device__ inline bool bar_wait(uint64_t *bar, uint32_t phase, long long attempts) {
     uint32_t addr = smem_u32(bar);
-    for (long long i = 0; i < kSpinLimit; i++) {
+    for (long long i = 0; i < attempts; i++) {
         uint32_t done;
         asm volatile("{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
                      "selp.b32 %0, 1, 0, P1;\n\t}\n" : "=r"(done) : "r"(addr), "r"(phase) : "memory");
@@ -247,16 +249,26 @@ __device__ inline void mma_tn(uint32_t d, const unsigned char *a, const unsigned
     }
 }
 
-// Issues with thread 0, commits to the barrier and waits (all threads).  Returns false on timeout.
+// Thread 0 commits the MMAs it issued to the barrier; every thread waits (bounded).  Returns, the
+// same in every thread of the CTA, whether all of them saw the MMAs complete.
 struct Sync {
     Scratch *h;
+    long long attempts;
     uint32_t phase = 0;
+    bool pending = false;       // this thread's wait ran out on phase pending_phase
+    uint32_t pending_phase = 0;
     __device__ bool wait_all() {
         if (threadIdx.x == 0) commit(&h->bar);
-        bool ok = bar_wait(&h->bar, phase);
+        bool ok = bar_wait(&h->bar, phase, attempts);
+        if (!ok) { pending = true; pending_phase = phase; }
         phase ^= 1;
+        ok = __syncthreads_and(ok) != 0;
         fence_after();
         return ok;
+    }
+    // after a wait that ran out: wait, with the full limit, for the committed MMAs to finish
+    __device__ void drain() {
+        if (pending) bar_wait(&h->bar, pending_phase, kSpinLimit);
     }
 };
 
@@ -289,7 +301,7 @@ __device__ inline bool group_sync_and(int id, bool ok) {
 __global__ void __launch_bounds__(kFwdThreads, kFwdCtasPerSm) forward_kernel(const unsigned char *weights,
                                                                              const pt_cache_query *queries, size_t count,
                                                                              const int32_t *count_dev, float3 lo, float3 hi,
-                                                                             float *out, int *status) {
+                                                                             float *out, int *status, long long attempts) {
     if (count_dev) count = min(count, size_t(max(0, *count_dev)));   // queue length known only on the device
     extern __shared__ __align__(1024) unsigned char smem[];
     Scratch *h = reinterpret_cast<Scratch *>(smem);
@@ -310,11 +322,12 @@ __global__ void __launch_bounds__(kFwdThreads, kFwdCtasPerSm) forward_kernel(con
     const uint32_t lane_col = tcol + ((uint32_t)((r & ~31u)) << 16);   // warp (w % 4) reads lanes 32 (w % 4) ..
     uint64_t *bar = &bars[g];
     const bool issuer = r == 0;
-    uint32_t phase = 0;
-    bool ok = true;
+    uint32_t phase = 0, pending_phase = 0;
+    bool ok = true, pending = false;
     auto wait_mma = [&]() {                       // commit this group's MMAs and wait for them (bounded)
         if (issuer) commit(bar);
-        bool done = bar_wait(bar, phase);
+        bool done = bar_wait(bar, phase, attempts);
+        if (!done) { pending = true; pending_phase = phase; }
         phase ^= 1;
         fence_after();
         return done;
@@ -356,6 +369,7 @@ __global__ void __launch_bounds__(kFwdThreads, kFwdCtasPerSm) forward_kernel(con
         ok = sync_group(done);                    // the next tile's MMAs write these TMEM columns again
     }
     if (!ok && r == 0) atomicExch(status, int(PT_TIMEOUT));
+    if (pending) bar_wait(bar, pending_phase, kSpinLimit);   // no MMA of this group may still write TMEM
     fence_before();
     __syncthreads();
     tmem_free(h->tmem, kFwdTmemCols);
@@ -369,7 +383,8 @@ constexpr size_t kTrainSmem = 256 + kWeightBytes + kPad + 6 * (kActBytes + kPad)
 
 __global__ void __launch_bounds__(kTile, 1) train_kernel(const unsigned char *weights, const pt_cache_query *queries,
                                                          const float *targets, size_t count, const int32_t *count_dev,
-                                                         float3 lo, float3 hi, float *partial, float *loss_partial, int *status) {
+                                                         float3 lo, float3 hi, float *partial, float *loss_partial, int *status,
+                                                         long long attempts) {
     if (count_dev) count = min(count, size_t(max(0, *count_dev)));
     const float grad_scale = count ? 1.0f / float(count * kOut) : 0.0f;   // mean over samples and channels
     extern __shared__ __align__(1024) unsigned char smem[];
@@ -390,7 +405,7 @@ __global__ void __launch_bounds__(kTile, 1) train_kernel(const unsigned char *we
     fence_after();
     const uint32_t tbase = h->tmem;
     const uint32_t lane_base = tbase + ((uint32_t)(threadIdx.x & ~31u) << 16);
-    Sync sync{h};
+    Sync sync{h, attempts};
     bool ok = true, first = true;
     float loss = 0.0f;
     const size_t tiles = (count + kTile - 1) / kTile;
@@ -493,6 +508,7 @@ __global__ void __launch_bounds__(kTile, 1) train_kernel(const unsigned char *we
     __syncthreads();
     if (threadIdx.x == 0) loss_partial[blockIdx.x] = warp_loss[0] + warp_loss[1] + warp_loss[2] + warp_loss[3];
     if (!ok && threadIdx.x == 0) atomicExch(status, int(PT_TIMEOUT));
+    sync.drain();                                 // no MMA may still write TMEM when it is freed
     fence_before();
     __syncthreads();
     tmem_free(tbase, 512);
@@ -502,8 +518,9 @@ __global__ void __launch_bounds__(kTile, 1) train_kernel(const unsigned char *we
 // loss partials into loss[0] (mean) and, for a training step (advance) on a non-empty batch,
 // advances the Adam step (step[0]) and the weight-average step (step[1]).
 __global__ void reduce_kernel(const float *partial, const float *loss_partial, int ctas, size_t count, const int32_t *count_dev,
-                              float *grad, float *loss, int *step, int advance) {
+                              float *grad, float *loss, int *step, int advance, const int *status) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (*status) return;                          // the gradients kernel timed out: no step
     if (i == 0) {
         size_t n = count_dev ? min(count, size_t(max(0, *count_dev))) : count;
         float l = 0.0f;
@@ -534,9 +551,9 @@ __host__ __device__ inline uint32_t master_to_canon(int i) {
 // moments are) and writes its bf16 copy, the weights that inference uses.
 __global__ void adam_kernel(float *master, float *m, float *v, const float *grad, const int *step_dev, const int32_t *count_dev,
                             float lr, float beta1, float beta2, float eps, unsigned char *canon_out, float ema_decay,
-                            float *ema, unsigned char *ema_canon) {
+                            float *ema, unsigned char *ema_canon, const int *status) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= kMasterFloats || (count_dev && *count_dev <= 0)) return;
+    if (i >= kMasterFloats || (count_dev && *count_dev <= 0) || *status) return;
     const int step = step_dev[0];
     float g = grad[i];
     float mi = beta1 * m[i] + (1.0f - beta1) * g;
@@ -573,6 +590,7 @@ struct pt_cache {
     int ctas = 0;
     float lr = 1e-2f, beta1 = 0.9f, beta2 = 0.99f, eps = 1e-8f;
     float ema_decay = 0.0f;
+    long long attempts = kSpinLimit;    // try_wait attempts per bounded wait (pt_cache_wait_limit)
     const unsigned char *inference() const { return (ema_decay > 0 ? ema_weights : weights).get<unsigned char>(); }
 };
 
@@ -601,11 +619,12 @@ void gradients(pt_cache *c, const pt_cache_query *q, const float *targets, size_
     size_t tiles = (count + kTile - 1) / kTile;
     int grid = count_dev ? c->ctas : int(std::min<size_t>(tiles ? tiles : 1, size_t(c->ctas)));
     train_kernel<<<grid, kTile, kTrainSmem, st>>>(c->weights.get<unsigned char>(), q, targets, count, count_dev, lo3(c), hi3(c),
-                                                   c->partial.get<float>(), c->loss_partial.get<float>(), c->status.get<int>());
+                                                   c->partial.get<float>(), c->loss_partial.get<float>(), c->status.get<int>(),
+                                                   c->attempts);
     PT_CUDA(cudaGetLastError());
     reduce_kernel<<<(kMasterFloats + 255) / 256, 256, 0, st>>>(c->partial.get<float>(), c->loss_partial.get<float>(), grid, count,
                                                                count_dev, c->grad.get<float>(), c->loss.get<float>(), c->step.get<int>(),
-                                                               advance ? 1 : 0);
+                                                               advance ? 1 : 0, c->status.get<int>());
     PT_CUDA(cudaGetLastError());
 }
 float read_loss(pt_cache *c, cudaStream_t st) {
@@ -626,7 +645,7 @@ void cache_forward(pt_cache *c, const pt_cache_query *queries, size_t count, con
     if (!tiles) return;
     int grid = int(std::min<size_t>((tiles + kFwdGroups - 1) / kFwdGroups, size_t(kFwdCtasPerSm) * size_t(c->ctas)));
     forward_kernel<<<grid, kFwdThreads, kFwdSmem, st>>>(c->inference(), queries, count, count_dev, lo3(c), hi3(c), rgb,
-                                                   c->status.get<int>());
+                                                   c->status.get<int>(), c->attempts);
     PT_CUDA(cudaGetLastError());
 }
 void cache_train(pt_cache *c, const pt_cache_query *queries, const float *targets, size_t count, const int32_t *count_dev,
@@ -636,7 +655,8 @@ void cache_train(pt_cache *c, const pt_cache_query *queries, const float *target
     adam_kernel<<<(kMasterFloats + 255) / 256, 256, 0, st>>>(c->master.get<float>(), c->adam_m.get<float>(), c->adam_v.get<float>(),
                                                              c->grad.get<float>(), c->step.get<int>(), count_dev, c->lr, c->beta1,
                                                              c->beta2, c->eps, c->weights.get<unsigned char>(), c->ema_decay,
-                                                             c->ema.get<float>(), c->ema_weights.get<unsigned char>());
+                                                             c->ema.get<float>(), c->ema_weights.get<unsigned char>(),
+                                                             c->status.get<int>());
     PT_CUDA(cudaGetLastError());
 }
 float cache_loss(pt_cache *c, cudaStream_t st) { return read_loss(c, st); }
@@ -721,6 +741,23 @@ pt_status pt_cache_train_device(pt_cache *c, const pt_cache_query *queries, cons
         cudaStream_t st = static_cast<cudaStream_t>(stream);
         cache_train(c, queries, targets, count, nullptr, st);
         if (loss) *loss = read_loss(c, st);
+    });
+}
+
+// Waits for `stream` and reports a timed-out tensor-core wait of an earlier call (clearing it).
+pt_status pt_cache_sync(pt_cache *c, void *stream) {
+    return guard([&]() {
+        if (!c) throw Error(PT_INVALID_ARGUMENT, "null cache");
+        PT_CUDA(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+        check_status(c);
+    });
+}
+
+// try_wait attempts per bounded tensor-core wait of this cache's kernels (< 0: the default).
+pt_status pt_cache_wait_limit(pt_cache *c, long long attempts) {
+    return guard([&]() {
+        if (!c) throw Error(PT_INVALID_ARGUMENT, "null cache");
+        c->attempts = attempts < 0 ? kSpinLimit : attempts;
     });
 }
 

@@ -6,6 +6,7 @@
 #include <cfloat>
 #include <algorithm>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include "pt_api_common.h"
 #include "pt_device.h"
@@ -147,6 +148,18 @@ __global__ void bounce_rays_kernel(DeviceScene s, const pt_ray *primary, const p
     out[k] = o;
 }
 
+// Surface rays (same arithmetic as pt_rays_surface on the host).
+__global__ void surface_rays_kernel(const pt_triangle *tris, uint64_t triangles, uint64_t seed, uint64_t first, size_t count,
+                                    pt_ray *rays, float *tmax) {
+    size_t k = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if(k >= count) return;
+    pt_ray o;
+    float hi = 0;
+    surface_ray(tris, triangles, seed, first + k, tmax != nullptr, o, &hi);
+    rays[k] = o;
+    if(tmax) tmax[k] = hi;
+}
+
 unsigned grid_for(size_t count, int block) { return unsigned((count + size_t(block) - 1) / size_t(block)); }
 
 // ---- ray ordering -----------------------------------------------------------------------------
@@ -211,14 +224,27 @@ const uint32_t *order_rays(const pt_scene *sc, const pt_ray *rays, size_t count,
 // Query kernel variant and its tunables (the autotuner sets these).
 QueryConfig g_query_config;
 
+// Resident blocks per SM of query-kernel variant `k` on `device` (the occupancy calculator's
+// answer, looked up once per device and variant).
+int blocks_per_sm(int device, int k, const void *fn, size_t smem) {
+    static std::mutex mutex;
+    static std::map<std::pair<int, int>, int> cache;
+    std::lock_guard<std::mutex> lock(mutex);
+    auto it = cache.find({device, k});
+    if (it != cache.end()) return it->second;
+    int n = 0;
+    PT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, kQueryBlock, smem));
+    cache[{device, k}] = n;
+    return n;
+}
+
 void launch_query(const pt_scene *sc, const pt_ray *rays, size_t count, int mode, float tmin, const float *tmax,
                   pt_hit *hits, pt_ray_stats *stats, int tie, cudaStream_t stream) {
     if(!count) return;
     const DeviceScene &s = sc->view;
     if(g_query_config.persistent) {
         pt_scene *m = const_cast<pt_scene *>(sc);
-        if(!m->ray_counter.bytes()) m->ray_counter.resize(sizeof(unsigned long long) * 64);
-        unsigned long long *counter = m->ray_counter.get<unsigned long long>() + (m->counter_slot++ % 64);
+        unsigned long long *counter = m->ray_counter.get<unsigned long long>() + (m->counter_slot.fetch_add(1) % kRayCounters);
         PT_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), stream));
         const bool wide = g_query_config.wide && s.nodes4;
         const bool any = mode == PT_QUERY_ANY;
@@ -232,10 +258,9 @@ void launch_query(const pt_scene *sc, const pt_ray *rays, size_t count, int mode
         int walk = wide ? (g_query_config.speculative ? 2 : 1) : 0;
         int k = (any ? 6 : 0) + (stats ? 3 : 0) + walk;
         Fn fn = table[k];
-        static int per_sm[12] = {0};
         const size_t smem = wide ? size_t(kSharedStack4) * kQueryBlock * sizeof(int2) : size_t(kSharedStack) * kQueryBlock * sizeof(int32_t);
-        if(!per_sm[k]) PT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[k], (const void *)fn, kQueryBlock, smem));
-        int bps = g_query_config.blocks_per_sm > 0 ? std::min(g_query_config.blocks_per_sm, per_sm[k]) : per_sm[k];
+        const int occupancy = blocks_per_sm(sc->device, k, (const void *)fn, smem);
+        int bps = g_query_config.blocks_per_sm > 0 ? std::min(g_query_config.blocks_per_sm, occupancy) : occupancy;
         size_t want = (count + kQueryBlock - 1) / kQueryBlock;
         unsigned grid = unsigned(std::min<size_t>(want, size_t(device_sm_count()) * size_t(bps > 0 ? bps : 1)));
         void *scratch = nullptr;
@@ -245,9 +270,16 @@ void launch_query(const pt_scene *sc, const pt_ray *rays, size_t count, int mode
             PT_CUDA(cudaStreamIsCapturing(stream, &capture));
             if (capture == cudaStreamCaptureStatusNone) order = order_rays(sc, rays, count, stream, scratch);   // not inside a graph capture
         }
+        cudaEvent_t *ev = nullptr;
+        if (!m->profile_events.empty()) {
+            const size_t pairs = m->profile_events.size() / 2;
+            ev = &m->profile_events[2 * (m->profile_next++ % pairs)];
+            PT_CUDA(cudaEventRecord(ev[0], stream));
+        }
         fn<<<grid, kQueryBlock, smem, stream>>>(s, rays, count, tmin, tmax, hits, stats, tie, counter, g_query_config.min_active,
                                                  order);
         PT_CUDA(cudaGetLastError());
+        if (ev) PT_CUDA(cudaEventRecord(ev[1], stream));
         if (scratch) PT_CUDA(cudaFreeAsync(scratch, stream));
         return;
     }
@@ -265,8 +297,10 @@ void launch_query(const pt_scene *sc, const pt_ray *rays, size_t count, int mode
 } // namespace ptb
 
 pt_scene::~pt_scene() {
+    for(auto &e : profile_events) cudaEventDestroy(e);
     for(auto &s : streams) if(s) cudaStreamDestroy(s);
-    if(order_pool) { cudaDeviceSynchronize(); cudaMemPoolDestroy(order_pool); }
+    // a pool destroyed with frees still pending on a stream is released once they complete
+    if(order_pool) cudaMemPoolDestroy(order_pool);
 }
 
 extern "C" {
@@ -318,6 +352,7 @@ pt_status pt_scene_create(const pt_scene_desc *desc, pt_scene **out) {
                 uint64_t keep = UINT64_MAX;
                 PT_CUDA(cudaMemPoolSetAttribute(sc->order_pool, cudaMemPoolAttrReleaseThreshold, &keep));
             }
+            sc->ray_counter.resize(sizeof(unsigned long long) * kRayCounters);
             sc->host_lights = lights;
             sc->light_area = area;
             sc->triangle_count = desc->triangle_count;
@@ -415,6 +450,7 @@ pt_status pt_query_rays(const pt_scene *cscene, const pt_ray *rays, size_t count
         if(!scene || (count && (!rays || !hits))) throw Error(PT_INVALID_ARGUMENT, "null argument");
         if(mode != PT_QUERY_CLOSEST && mode != PT_QUERY_ANY) throw Error(PT_INVALID_ARGUMENT, "unknown query mode");
         if(!count) return;
+        std::lock_guard<std::mutex> lock(scene->work_mutex);   // the staging buffers are the scene's
         const size_t chunk = size_t(1) << 22;
         size_t per = count < chunk ? count : chunk;
         for(int k = 0; k < 3; k++) {
@@ -482,6 +518,39 @@ pt_status pt_query_order(int enabled) {
     return guard([&]() { g_query_config.order = enabled ? 1 : 0; });
 }
 
+// Walk-kernel timing: `launches` > 0 creates that many event pairs (recorded around each later
+// walk-kernel launch of this scene, a ring); 0 removes them.
+pt_status pt_query_profile(pt_scene *scene, int launches) {
+    return guard([&]() {
+        if(!scene || launches < 0) throw Error(PT_INVALID_ARGUMENT, "invalid profile arguments");
+        PT_CUDA(cudaDeviceSynchronize());
+        for(auto &e : scene->profile_events) cudaEventDestroy(e);
+        scene->profile_events.clear();
+        scene->profile_next = 0;
+        for(int k = 0; k < 2 * launches; k++) {
+            cudaEvent_t e;
+            PT_CUDA(cudaEventCreate(&e));
+            scene->profile_events.push_back(e);
+        }
+    });
+}
+
+// Durations (ms) of the walk launches recorded since pt_query_profile, oldest first (at most the
+// ring's size); waits for the last one.
+pt_status pt_query_profile_read(pt_scene *scene, float *ms, size_t capacity, size_t *count) {
+    return guard([&]() {
+        if(!scene || !count) throw Error(PT_INVALID_ARGUMENT, "null argument");
+        const size_t pairs = scene->profile_events.size() / 2;
+        const size_t n = std::min(scene->profile_next, pairs);
+        *count = n;
+        for(size_t k = 0; k < n && k < capacity; k++) {
+            size_t slot = (scene->profile_next - n + k) % pairs;
+            PT_CUDA(cudaEventSynchronize(scene->profile_events[2 * slot + 1]));
+            PT_CUDA(cudaEventElapsedTime(&ms[k], scene->profile_events[2 * slot], scene->profile_events[2 * slot + 1]));
+        }
+    });
+}
+
 // ---- no-allocation query ---------------------------------------------------------------------
 // Scratch of pt_query_rays_static, shared by every call on a device: the persistent kernel's
 // ray counter, then staging for PT_STATIC_QUERY_MAX_RAYS rays, tmax values, hits and counters.
@@ -539,22 +608,26 @@ pt_status pt_query_rays_static(const pt_scene *scene, const pt_ray *rays, size_t
         if(tmax) PT_CUDA(cudaMemcpyAsync(d_tmax, tmax, count * sizeof(float), cudaMemcpyHostToDevice, st));
         PT_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st));   // the counter must start at zero
         const DeviceScene &s = scene->view;
-        const bool wide = s.nodes4 != nullptr;
+        const bool wide = g_query_config.wide && s.nodes4 != nullptr;
         const bool any = mode == PT_QUERY_ANY;
+        const int walk = wide ? (g_query_config.speculative ? 2 : 1) : 0;
         using Fn = void (*)(DeviceScene, const pt_ray *, size_t, float, const float *, pt_hit *, pt_ray_stats *, int,
                             unsigned long long *, int, const uint32_t *);
-        static const Fn table[8] = {
-            query_persistent_kernel<false, false, 0>, query_persistent_kernel<false, false, 2>,
-            query_persistent_kernel<false, true, 0>, query_persistent_kernel<false, true, 2>,
-            query_persistent_kernel<true, false, 0>, query_persistent_kernel<true, false, 2>,
-            query_persistent_kernel<true, true, 0>, query_persistent_kernel<true, true, 2>};
-        Fn fn = table[(any ? 4 : 0) + (stats ? 2 : 0) + (wide ? 1 : 0)];
+        static const Fn table[12] = {
+            query_persistent_kernel<false, false, 0>, query_persistent_kernel<false, false, 1>, query_persistent_kernel<false, false, 2>,
+            query_persistent_kernel<false, true, 0>, query_persistent_kernel<false, true, 1>, query_persistent_kernel<false, true, 2>,
+            query_persistent_kernel<true, false, 0>, query_persistent_kernel<true, false, 1>, query_persistent_kernel<true, false, 2>,
+            query_persistent_kernel<true, true, 0>, query_persistent_kernel<true, true, 1>, query_persistent_kernel<true, true, 2>};
+        const int k = (any ? 6 : 0) + (stats ? 3 : 0) + walk;
+        Fn fn = table[k];
         const size_t smem = wide ? size_t(kSharedStack4) * kQueryBlock * sizeof(int2) : size_t(kSharedStack) * kQueryBlock * sizeof(int32_t);
-        int per_sm = 0;
-        PT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)fn, kQueryBlock, smem));
+        int dev = 0;
+        PT_CUDA(cudaGetDevice(&dev));
+        const int per_sm = blocks_per_sm(dev, k, (const void *)fn, smem);
         size_t want = (count + kQueryBlock - 1) / kQueryBlock;
         unsigned grid = unsigned(std::min<size_t>(want, size_t(device_sm_count()) * size_t(per_sm > 0 ? per_sm : 1)));
-        fn<<<grid, kQueryBlock, smem, st>>>(s, d_rays, count, tmin, d_tmax, d_hits, d_stats, kTieLowestId, counter, 16, nullptr);
+        fn<<<grid, kQueryBlock, smem, st>>>(s, d_rays, count, tmin, d_tmax, d_hits, d_stats, kTieLowestId, counter,
+                                            g_query_config.min_active, nullptr);
         PT_CUDA(cudaGetLastError());
         PT_CUDA(cudaMemcpyAsync(hits, d_hits, count * sizeof(pt_hit), cudaMemcpyDeviceToHost, st));
         if(stats) PT_CUDA(cudaMemcpyAsync(stats, d_stats, count * sizeof(pt_ray_stats), cudaMemcpyDeviceToHost, st));
@@ -580,6 +653,18 @@ pt_status pt_rays_bounce_device(const pt_scene *scene, const pt_ray *primary, co
         if(!scene->triangle_count) throw Error(PT_INVALID_ARGUMENT, "bounce rays need triangles");
         bounce_rays_kernel<<<grid_for(count, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(scene->view, primary, hits, count, seed,
                                                                                                  first, scene->triangle_count, out);
+        PT_CUDA(cudaGetLastError());
+    });
+}
+
+pt_status pt_rays_surface_device(const pt_scene *scene, uint64_t seed, uint64_t first, size_t count, pt_ray *rays,
+                                 float *shadow_tmax, void *stream) {
+    return guard([&]() {
+        if(!scene || (count && !rays)) throw Error(PT_INVALID_ARGUMENT, "null argument");
+        if(!count) return;
+        if(!scene->triangle_count) throw Error(PT_INVALID_ARGUMENT, "surface rays need triangles");
+        surface_rays_kernel<<<grid_for(count, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+            scene->view.triangles, scene->triangle_count, seed, first, count, rays, shadow_tmax);
         PT_CUDA(cudaGetLastError());
     });
 }

@@ -325,6 +325,19 @@ pt_status pt_rays_camera(const pt_camera *camera, int width, int height, uint64_
     });
 }
 
+// The camera rays of pt_rays_camera with the given ray indices (index[k] in place of first + k).
+pt_status pt_rays_camera_at(const pt_camera *camera, int width, int height, uint64_t seed, const uint64_t *index,
+                            size_t count, pt_ray *rays) {
+    return guard([&]() {
+        if(!camera || (count && (!rays || !index)) || width <= 0 || height <= 0)
+            throw Error(PT_INVALID_ARGUMENT, "invalid camera ray arguments");
+        for(size_t k = 0; k < count; k++) {
+            pt_status st = pt_rays_camera(camera, width, height, seed, index[k], 1, rays + k);
+            if(st != PT_OK) throw Error(st, pt_last_error());
+        }
+    });
+}
+
 } // extern "C"
 
 
@@ -335,58 +348,54 @@ extern "C" pt_status pt_rays_surface(const pt_flat *scene, uint64_t seed, uint64
         const auto &T = scene->scene.triangles;
         if(T.empty()) throw Error(PT_INVALID_ARGUMENT, "surface rays need triangles");
         uint64_t ntri = T.size();
-        auto point = [&](Pcg &r, f3 &p, f3 &n) { surface_point(T.data(), ntri, r, p, n); };
         int nt = threads > 0 ? threads : hardware_threads();
         if(size_t(nt) > count / 4096 + 1) nt = int(count / 4096 + 1);
         std::vector<std::thread> pool;
         for(int t = 0; t < nt; t++) {
             size_t b = count * size_t(t) / size_t(nt), e = count * size_t(t + 1) / size_t(nt);
             pool.emplace_back([&, b, e]() {
-                for(size_t k = b; k < e; k++) {
-                    Pcg r; r.seed(seed, first + k);
-                    f3 p, n;
-                    point(r, p, n);
-                    pt_ray &out = rays[k];
-                    out.origin = pv(p); out.time = 0;
-                    if(shadow_tmax) {
-                        f3 q, m;
-                        point(r, q, m);
-                        f3 d = q - p;
-                        float dist = length(d);
-                        out.direction = pv(dist > 0 ? d / dist : n);
-                        shadow_tmax[k] = dist > 0.002f ? dist - 0.001f : 0.001f;
-                    } else {
-                        out.direction = pv(cosine_lift(n, r));
-                    }
-                }
+                for(size_t k = b; k < e; k++)
+                    surface_ray(T.data(), ntri, seed, first + k, shadow_tmax != nullptr, rays[k], shadow_tmax ? shadow_tmax + k : nullptr);
             });
         }
         for(auto &th : pool) th.join();
     });
 }
 
+static void bounce_rays_host(const pt_flat *scene, const pt_ray *primary, const pt_hit *hits, size_t count, uint64_t seed,
+                             uint64_t first, const uint64_t *streams, pt_ray *rays, int threads) {
+    if(!scene || (count && (!primary || !hits || !rays))) throw Error(PT_INVALID_ARGUMENT, "invalid bounce ray arguments");
+    const auto &T = scene->scene.triangles;
+    const auto &S = scene->scene.spheres;
+    if(T.empty()) throw Error(PT_INVALID_ARGUMENT, "bounce rays need triangles");
+    for(size_t k = 0; k < count; k++) {
+        const pt_hit &h = hits[k];
+        if((h.primitive_type == PT_TRIANGLE && (h.primitive_id < 0 || size_t(h.primitive_id) >= T.size())) ||
+           (h.primitive_type == PT_SPHERE && (h.primitive_id < 0 || size_t(h.primitive_id) >= S.size())))
+            throw Error(PT_INVALID_ARGUMENT, "hit refers to a primitive outside the scene");
+    }
+    int nt = threads > 0 ? threads : hardware_threads();
+    if(size_t(nt) > count / 4096 + 1) nt = int(count / 4096 + 1);
+    std::vector<std::thread> pool;
+    for(int t = 0; t < nt; t++) {
+        size_t b = count * size_t(t) / size_t(nt), e = count * size_t(t + 1) / size_t(nt);
+        pool.emplace_back([&, b, e]() {
+            for(size_t k = b; k < e; k++)
+                bounce_ray(T.data(), T.size(), S.data(), primary[k], hits[k], seed, streams ? streams[k] : first + k, rays[k]);
+        });
+    }
+    for(auto &th : pool) th.join();
+}
+
 extern "C" pt_status pt_rays_bounce(const pt_flat *scene, const pt_ray *primary, const pt_hit *hits, size_t count,
                                     uint64_t seed, uint64_t first, pt_ray *rays, int threads) {
+    return guard([&]() { bounce_rays_host(scene, primary, hits, count, seed, first, nullptr, rays, threads); });
+}
+
+extern "C" pt_status pt_rays_bounce_at(const pt_flat *scene, const pt_ray *primary, const pt_hit *hits, size_t count,
+                                       uint64_t seed, const uint64_t *streams, pt_ray *rays, int threads) {
     return guard([&]() {
-        if(!scene || (count && (!primary || !hits || !rays))) throw Error(PT_INVALID_ARGUMENT, "invalid bounce ray arguments");
-        const auto &T = scene->scene.triangles;
-        const auto &S = scene->scene.spheres;
-        if(T.empty()) throw Error(PT_INVALID_ARGUMENT, "bounce rays need triangles");
-        for(size_t k = 0; k < count; k++) {
-            const pt_hit &h = hits[k];
-            if((h.primitive_type == PT_TRIANGLE && (h.primitive_id < 0 || size_t(h.primitive_id) >= T.size())) ||
-               (h.primitive_type == PT_SPHERE && (h.primitive_id < 0 || size_t(h.primitive_id) >= S.size())))
-                throw Error(PT_INVALID_ARGUMENT, "hit refers to a primitive outside the scene");
-        }
-        int nt = threads > 0 ? threads : hardware_threads();
-        if(size_t(nt) > count / 4096 + 1) nt = int(count / 4096 + 1);
-        std::vector<std::thread> pool;
-        for(int t = 0; t < nt; t++) {
-            size_t b = count * size_t(t) / size_t(nt), e = count * size_t(t + 1) / size_t(nt);
-            pool.emplace_back([&, b, e]() {
-                for(size_t k = b; k < e; k++) bounce_ray(T.data(), T.size(), S.data(), primary[k], hits[k], seed, first + k, rays[k]);
-            });
-        }
-        for(auto &th : pool) th.join();
+        if(count && !streams) throw Error(PT_INVALID_ARGUMENT, "null stream indices");
+        bounce_rays_host(scene, primary, hits, count, seed, 0, streams, rays, threads);
     });
 }

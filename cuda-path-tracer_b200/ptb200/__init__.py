@@ -119,8 +119,14 @@ def library() -> C.CDLL:
         "pt_query_layout": (I, [I]),
         "pt_query_walk": (I, [I]),
         "pt_query_order": (I, [I]),
+        "pt_query_profile": (I, [P, I]),
+        "pt_query_profile_read": (I, [P, P, S, P]),
+        "pt_probe_read_bandwidth": (I, [S, I, P]),
         "pt_rays_camera_device": (I, [P, I, I, U64, U64, S, P, P]),
         "pt_rays_bounce_device": (I, [P, P, P, S, U64, U64, P, P]),
+        "pt_rays_surface_device": (I, [P, U64, U64, S, P, P, P]),
+        "pt_rays_camera_at": (I, [P, I, I, U64, P, S, P]),
+        "pt_rays_bounce_at": (I, [P, P, P, S, U64, P, P, I]),
         "pt_flat_from_desc": (I, [P, P]),
         "pt_flat_build_bvh": (I, [P, I]),
         "pt_flat_desc": (I, [P, P]),
@@ -153,6 +159,7 @@ def library() -> C.CDLL:
         "pt_batch_stats": (I, [P, P, P, P, S]),
         "pt_batch_tuning": (I, [P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
         "pt_batch_autotune": (I, [P, C.c_int32, C.c_char_p, P]),
+        "pt_batch_fail_probe": (I, [P, C.c_int32]),
         "pt_cache_create": (I, [P, P, U64, P]),
         "pt_cache_destroy": (I, [P]),
         "pt_cache_query_device": (I, [P, P, S, P, P]),
@@ -161,6 +168,8 @@ def library() -> C.CDLL:
         "pt_cache_weights": (I, [P, P, P, S]),
         "pt_cache_hyper": (I, [P, F, F, F, F]),
         "pt_cache_average": (I, [P, F]),
+        "pt_cache_sync": (I, [P, P]),
+        "pt_cache_wait_limit": (I, [P, C.c_longlong]),
         "pt_cached_defaults": (I, [P]),
         "pt_cached_create": (I, [P, P, C.c_int, C.c_int, U64, C.c_int, P, P]),
         "pt_cached_destroy": (I, [P]),
@@ -342,6 +351,14 @@ def camera_rays(camera: np.ndarray, width: int, height: int, seed: int, first: i
     return out
 
 
+def camera_rays_at(camera: np.ndarray, width: int, height: int, seed: int, index) -> np.ndarray:
+    """The camera rays of camera_rays with the given ray indices (pt_rays_camera_at)."""
+    index = np.ascontiguousarray(index, np.uint64)
+    out = np.zeros(len(index), RAY)
+    check(library().pt_rays_camera_at(camera.ctypes.data, width, height, seed, _ptr(index), len(index), _ptr(out)))
+    return out
+
+
 def surface_rays(scene: FlatScene, seed: int, first: int, count: int, shadow: bool = False, threads: int = 0):
     lib = library()
     h = C.c_void_p()
@@ -368,6 +385,24 @@ def bounce_rays(scene: FlatScene, primary: np.ndarray, hits: np.ndarray, seed: i
         hits = np.ascontiguousarray(hits, HIT)
         out = np.zeros(len(primary), RAY)
         check(lib.pt_rays_bounce(h, _ptr(primary), _ptr(hits), len(primary), seed, first, _ptr(out), threads))
+        return out
+    finally:
+        lib.pt_flat_destroy(h)
+
+
+def bounce_rays_at(scene: FlatScene, primary: np.ndarray, hits: np.ndarray, seed: int, streams,
+                   threads: int = 0) -> np.ndarray:
+    """bounce_rays with an explicit PCG stream index per ray (pt_rays_bounce_at)."""
+    lib = library()
+    h = C.c_void_p()
+    d = scene.desc()
+    check(lib.pt_flat_from_desc(C.byref(d), C.byref(h)))
+    try:
+        primary = np.ascontiguousarray(primary, RAY)
+        hits = np.ascontiguousarray(hits, HIT)
+        streams = np.ascontiguousarray(streams, np.uint64)
+        out = np.zeros(len(primary), RAY)
+        check(lib.pt_rays_bounce_at(h, _ptr(primary), _ptr(hits), len(primary), seed, _ptr(streams), _ptr(out), threads))
         return out
     finally:
         lib.pt_flat_destroy(h)
@@ -432,12 +467,36 @@ class Scene:
         check(library().pt_query_rays_compat(self._h, _ptr(rays), len(rays), int(brute), _ptr(out)))
         return out
 
+    def profile(self, launches: int) -> None:
+        """Records CUDA events around the next walk-kernel launches (a ring of `launches`; 0 stops)."""
+        check(library().pt_query_profile(self._h, launches))
+
+    def profile_read(self) -> np.ndarray:
+        """Durations (ms) of the walk launches recorded since profile(), oldest first."""
+        n = C.c_size_t()
+        check(library().pt_query_profile_read(self._h, None, 0, C.byref(n)))
+        out = np.zeros(n.value, np.float32)
+        check(library().pt_query_profile_read(self._h, _ptr(out), n.value, C.byref(n)))
+        return out
+
     def bounce_rays_device(self, primary, hits, count: int, seed: int, first: int, out, stream=0):
         check(library().pt_rays_bounce_device(self._h, _ptr(primary), _ptr(hits), count, seed, first, _ptr(out), stream))
 
 
+    def surface_rays_device(self, seed: int, first: int, count: int, out, tmax=None, stream=0):
+        """Surface rays (or, with tmax, shadow rays between surface points) on the device."""
+        check(library().pt_rays_surface_device(self._h, seed, first, count, _ptr(out), _ptr(tmax), stream))
+
+
 def camera_rays_device(camera: np.ndarray, width, height, seed, first, count, out, stream=0):
     check(library().pt_rays_camera_device(camera.ctypes.data, width, height, seed, first, count, _ptr(out), stream))
+
+
+def read_bandwidth(nbytes: int, reps: int = 20) -> float:
+    """GB/s of 16-byte loads over a buffer of nbytes (pt_probe_read_bandwidth)."""
+    g = C.c_float()
+    check(library().pt_probe_read_bandwidth(nbytes, reps, C.byref(g)))
+    return g.value
 
 
 def query_tuning(persistent: int = 1, min_active: int = 8, blocks_per_sm: int = 0) -> None:
@@ -679,6 +738,14 @@ class RadianceCache:
 
     def hyper(self, lr=1e-2, beta1=0.9, beta2=0.99, eps=1e-8) -> None:
         check(library().pt_cache_hyper(self._h, lr, beta1, beta2, eps))
+
+    def sync(self, stream=0) -> None:
+        """Waits for `stream`; raises PtError (status PT_TIMEOUT) if a tensor-core wait ran out."""
+        check(library().pt_cache_sync(self._h, stream))
+
+    def wait_limit(self, attempts: int) -> None:
+        """try_wait attempts per bounded wait (< 0: the default; 0: every wait runs out at once)."""
+        check(library().pt_cache_wait_limit(self._h, attempts))
 
     def average(self, decay: float) -> None:
         """Queries use a bias-corrected moving average of the weights (decay 0: the weights)."""

@@ -35,7 +35,11 @@ typedef enum pt_status {
     PT_INVALID_ARGUMENT = 1, /* std::invalid_argument in the reference (bad dims, sample counts, block shapes) */
     PT_INVALID_SCENE = 2,    /* std::runtime_error("invalid flat scene data"), src/flat/flat_validate.h:12 */
     PT_CUDA_ERROR = 3,       /* std::runtime_error from a failing CUDA call, src/cuda/cuda_renderer.cu:8-11 */
-    PT_STACK_OVERFLOW = 4,   /* "CUDA traversal stack overflow", src/cuda/cuda_renderer.cu:204 */
+    PT_STACK_OVERFLOW = 4,   /* "CUDA traversal stack overflow", src/cuda/cuda_renderer.cu:204.  trace_world's
+                              * stack holds 64 entries and validate_flat_scene bounds a tree's depth at 64,
+                              * which keeps it from overflowing (a level leaves at most one entry behind);
+                              * this library's walks keep at most 63 (two-wide) or 3 per four-wide level
+                              * (192 entries), so a scene pt_scene_create accepts never reports it either */
     PT_QUEUE_OVERFLOW = 5,   /* a wavefront queue would exceed its capacity */
     PT_TIMEOUT = 6,          /* a bounded device-side wait ran out */
     PT_NO_DEVICE = 7         /* cuda_device_available() == false; the CLI exits 77 */
@@ -127,18 +131,24 @@ pt_status pt_scene_device_bytes(const pt_scene *scene, size_t *bytes);
  * (src/renderer/transport.h:206-209). */
 enum { PT_QUERY_CLOSEST = 0, PT_QUERY_ANY = 1 };
 /* Device buffers, asynchronous on `stream` (a cudaStream_t; 0 = legacy default stream).
- * `tmax` may be NULL (FLT_MAX for every ray); `stats` may be NULL. */
+ * `tmax` may be NULL (FLT_MAX for every ray); `stats` may be NULL.  Several host threads may query
+ * one scene; each launch takes one of the scene's 64 ray counters in turn, so at most 64 queries of
+ * one scene may be in flight on the GPU at once. */
 pt_status pt_query_rays_device(const pt_scene *scene, const pt_ray *rays, size_t count, int mode,
                                float tmin, const float *tmax, pt_hit *hits, pt_ray_stats *stats,
                                void *stream);
-/* Host buffers: uploads, traces and downloads in overlapped chunks; returns when `hits` is filled. */
+/* Host buffers: uploads, traces and downloads in overlapped chunks; returns when `hits` is filled.
+ * Calls on one scene from several host threads take turns (the staging buffers are the scene's). */
 pt_status pt_query_rays(const pt_scene *scene, const pt_ray *rays, size_t count, int mode,
                         float tmin, const float *tmax, pt_hit *hits, pt_ray_stats *stats);
 /* Host-buffer query that allocates nothing.  Some callers cannot let a library call cudaMalloc
  * or cudaFree: applications that hand all device memory to their own pool allocator at start-up,
  * latency-critical loops (cudaFree can synchronize the whole device and stall other streams),
  * and processes running under a device-memory cap where a late allocation may fail.
- * No counterpart in the reference.  It answers exactly like pt_query_rays but stages the rays,
+ * No counterpart in the reference.  It walks with the process-wide settings of pt_query_layout,
+ * pt_query_walk and pt_query_tuning (never in key order: see pt_query_order) and gives the
+ * answers of pt_query_rays (the per-ray counters of a persistent walk depend on which rays share
+ * a warp, so they may differ between calls).  It stages the rays,
  * tmax values, hits and counters through one static device array of the library (about 3.7 MB,
  * held by every GPU that loads the library until the process exits), so a call takes at most
  * PT_STATIC_QUERY_MAX_RAYS rays (more is PT_INVALID_ARGUMENT) and waits for its own work on
@@ -178,6 +188,15 @@ pt_status pt_query_walk(int speculative);
  * taken as given.  Results do not depend on it.  pt_query_rays_static never reorders. */
 pt_status pt_query_order(int enabled);
 
+/* Timing of the traversal kernel alone: launches > 0 records a pair of CUDA events around each
+ * of the scene's next walk-kernel launches (a ring of `launches` pairs; 0 stops recording), and
+ * pt_query_profile_read returns their durations in ms, oldest first (waits for the last one). */
+pt_status pt_query_profile(pt_scene *scene, int launches);
+pt_status pt_query_profile_read(pt_scene *scene, float *ms, size_t capacity, size_t *count);
+/* Read bandwidth of this GPU in GB/s for a buffer of `bytes` read `reps` times with 16-byte loads
+ * (under the L2 size: L2 bandwidth; several GB: HBM); allocates and frees the buffer. */
+pt_status pt_probe_read_bandwidth(size_t bytes, int reps, float *gbs);
+
 /* ---- device ray generators (bit-identical to the host ones in pt_workloads.h) ----
  * Camera rays of pt_rays_camera; bounce rays from closest hits: origin at the hit, a
  * cosine-distributed direction about the geometric normal turned toward the ray, one PCG stream
@@ -186,6 +205,10 @@ pt_status pt_rays_camera_device(const pt_camera *camera, int width, int height, 
                                 size_t count, pt_ray *rays, void *stream);
 pt_status pt_rays_bounce_device(const pt_scene *scene, const pt_ray *primary, const pt_hit *hits, size_t count,
                                 uint64_t seed, uint64_t first, pt_ray *rays, void *stream);
+/* Surface rays of pt_rays_surface (pt_workloads.h) on the device: stream (seed, first + k) per ray;
+ * shadow_tmax non-NULL: shadow rays between two surface points with shadow_tmax[k] = distance - 0.001. */
+pt_status pt_rays_surface_device(const pt_scene *scene, uint64_t seed, uint64_t first, size_t count, pt_ray *rays,
+                                 float *shadow_tmax, void *stream);
 
 /* ---- progressive renderer ----
  * Replaces class cuda_renderer (src/cuda/cuda_renderer.h:10-29).  `flags` is a bit set of
@@ -250,8 +273,13 @@ pt_status pt_batch_tuning(pt_batch *batch, int32_t path_capacity, int32_t block,
                           int32_t use_graph);
 /* Sweeps capacity x block x min_active x graph on probe runs (each job at min(probe_samples, its
  * samples)), applies the fastest and caches it per (log2 triangles, log2 pixels) bucket in
- * `cache_path` (NULL: no cache).  best = {capacity, block, min_active, use_graph}. */
+ * `cache_path` (NULL: no cache).  best = {capacity, block, min_active, use_graph}.  A probe run that
+ * fails (timeout, stack overflow) skips its setting; the jobs' sample counts are restored whatever
+ * happens; a CUDA error ends the sweep with PT_CUDA_ERROR. */
 pt_status pt_batch_autotune(pt_batch *batch, int32_t probe_samples, const char *cache_path, int32_t *best);
+/* Fault injection for tests, on the host: the n-th probe run of the next pt_batch_autotune fails as a
+ * timed-out run would (the sweep skips that setting; the jobs keep their sample counts); n <= 0: none. */
+pt_status pt_batch_fail_probe(pt_batch *batch, int32_t n);
 
 /* ---- learned radiance cache ----
  * A small MLP (64 encoded inputs -> 5 hidden layers of 64, ReLU -> 3 outputs, exp) trained
@@ -275,6 +303,14 @@ pt_status pt_cache_train_device(pt_cache *cache, const pt_cache_query *queries, 
 /* The gradient of the mean loss w.r.t. the FP32 masters (host buffer of PT_CACHE_WEIGHTS), no update. */
 pt_status pt_cache_gradients(pt_cache *cache, const pt_cache_query *queries, const float *targets, size_t count,
                              float *grad, float *loss);
+/* Waits for `stream`; returns PT_TIMEOUT (and clears it) when a tensor-core wait of an earlier
+ * asynchronous call of this cache ran out (its outputs are then not valid and no Adam step was
+ * applied).  Every wait of the cache's kernels is bounded; after one runs out the kernel waits once
+ * more, with the full bound, for the tensor-core work it had issued, frees its TMEM and returns. */
+pt_status pt_cache_sync(pt_cache *cache, void *stream);
+/* try_wait attempts per bounded wait of this cache's kernels (< 0: the default, 2^22).  0 makes every
+ * wait run out at once: fault injection for tests of the PT_TIMEOUT path. */
+pt_status pt_cache_wait_limit(pt_cache *cache, long long attempts);
 /* Reads (get != NULL) and/or replaces (set != NULL) the FP32 master weights. */
 pt_status pt_cache_weights(pt_cache *cache, float *get, const float *set, size_t floats);
 /* Adam hyper-parameters (defaults 1e-2, 0.9, 0.99, 1e-8). */

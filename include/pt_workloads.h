@@ -86,11 +86,19 @@ pt_status pt_rays_camera(const pt_camera *camera, int width, int height, uint64_
 pt_status pt_rays_surface(const pt_flat *scene, uint64_t seed, uint64_t first, size_t count,
                           pt_ray *rays, float *shadow_tmax, int threads);
 
+/* pt_rays_camera for arbitrary ray indices: rays[k] is the camera ray with index[k] (a random
+ * sample of a larger ray set, for bounded CPU checks and baselines). */
+pt_status pt_rays_camera_at(const pt_camera *camera, int width, int height, uint64_t seed, const uint64_t *index,
+                            size_t count, pt_ray *rays);
+
 /* Bounce rays from closest hits (host form of pt_rays_bounce_device, bit-identical): origin at
  * the hit, a cosine-distributed direction about the geometric normal turned toward the ray, PCG
  * stream (seed, first + k); a miss becomes a random surface ray. */
 pt_status pt_rays_bounce(const pt_flat *scene, const pt_ray *primary, const pt_hit *hits, size_t count,
                          uint64_t seed, uint64_t first, pt_ray *rays, int threads);
+/* pt_rays_bounce with an explicit PCG stream index per ray (streams[k] in place of first + k). */
+pt_status pt_rays_bounce_at(const pt_flat *scene, const pt_ray *primary, const pt_hit *hits, size_t count,
+                            uint64_t seed, const uint64_t *streams, pt_ray *rays, int threads);
 
 #ifdef __cplusplus
 }

@@ -51,6 +51,7 @@ class Oracle:
             "or_sphere_hit": (I, [P, P, F, F, P]),
             "or_trace_world": (I, [P, P, F, F, P, I, I, P, P, P]),
             "or_query": (None, [P, P, S, I, F, P, I, I, P, P, I]),
+            "or_query_ties": (None, [P, P, S, I, F, P, I, I, P, P, P, I]),
             "or_query_compat": (None, [P, P, S, I, P, I]),
             "or_add_samples": (I, [P, P, I, I, I, I, I, I, I, P, P, P, I]),
             "or_reset": (None, [I, I, U64, P, P]),
@@ -97,6 +98,18 @@ class Oracle:
         self.lib.or_query(C.byref(v), _p(rays), len(rays), mode, tmin, _p(tm), int(brute), int(tie_lowest), _p(hits),
                           _p(st), nthreads or threads())
         return (hits, st) if stats else hits
+
+    def query_ties(self, scene, rays, mode=pt.QUERY_CLOSEST, tmin=0.001, tmax=None, nthreads=None):
+        """Closest (lowest-id ties) or any hit, plus per ray how many other primitives were hit
+        at exactly the closest distance: (hits, ties)."""
+        v = self.view(scene, with_lights=False)
+        rays = np.ascontiguousarray(rays, pt.RAY)
+        hits = np.zeros(len(rays), pt.HIT)
+        ties = np.zeros(len(rays), np.int32)
+        tm = None if tmax is None else np.ascontiguousarray(tmax, np.float32)
+        self.lib.or_query_ties(C.byref(v), _p(rays), len(rays), mode, tmin, _p(tm), 0, 1, _p(hits), None, _p(ties),
+                               nthreads or threads())
+        return hits, ties
 
     def query_compat(self, scene, rays, brute=False):
         v = self.view(scene, with_lights=False)
@@ -279,6 +292,57 @@ class RefCpu:
             return t
         finally:
             self.lib.ref_mesh_free(h)
+
+
+class RefMesh:
+    """The reference's pre-CUDA host path: its triangle objects under its own bvh_node (random-axis
+    median split, drand48 seeded), hit through the virtual hittable::hit, as
+    tests/mesh_validation.cpp:76-81 does.  Built once; hits() timed separately."""
+
+    def __init__(self, ref: RefCpu, vertices, seed: int = 7):
+        self.ref = ref
+        v = np.ascontiguousarray(vertices, np.float32).reshape(-1, 3, 3)
+        self.h = ref.lib.ref_mesh_create(_p(v), len(v), seed)
+        if not self.h:
+            raise RuntimeError("ref_mesh_create failed")
+
+    def hits(self, rays, tmin=0.001, nthreads=None):
+        """t of the closest hit per ray (-1 on a miss)."""
+        rays = np.ascontiguousarray(rays, pt.RAY)
+        t = np.zeros(len(rays), np.float32)
+        self.ref.lib.ref_mesh_hit(self.h, _p(rays), len(rays), tmin, _p(t), nthreads or threads())
+        return t
+
+    def close(self):
+        if self.h:
+            self.ref.lib.ref_mesh_free(self.h)
+            self.h = None
+
+
+REF_TIMING_SO = REF_GPU_SO.with_name("libref_cuda_timing.so")
+
+
+class RefGpuTiming:
+    """Device time of the reference's own query_rays kernel (oracle/ref_cuda_timing.cu): the scene
+    uploaded by its device_scene, rays already on the device, CUDA events around the launches."""
+
+    def __init__(self):
+        if not REF_TIMING_SO.exists():
+            raise RuntimeError(f"{REF_TIMING_SO} is not built (make -C oracle ref)")
+        lib = C.CDLL(str(REF_TIMING_SO))
+        lib.reftime_last_error.restype, lib.reftime_last_error.argtypes = C.c_char_p, []
+        lib.reftime_query.restype = I
+        lib.reftime_query.argtypes = [P, P, S, I, I, P, P, S]
+        self.lib = lib
+
+    def query(self, scene, device_rays: int, count: int, warmup: int = 1, reps: int = 3, sample: int = 0):
+        """(mean kernel ms, the first `sample` trace_result records of the last launch)."""
+        d = scene.desc()
+        ms = C.c_float()
+        out = np.zeros(sample, pt.TRACE_RESULT)
+        if self.lib.reftime_query(C.byref(d), device_rays, count, warmup, reps, C.byref(ms), _p(out), sample):
+            raise RuntimeError(self.lib.reftime_last_error().decode())
+        return ms.value, out
 
 
 def ref_gpu_so(depth=None) -> Path:

@@ -196,9 +196,13 @@ static inline int lower_key(const pt_flat_hit *a, const pt_flat_hit *b) {
     return a->primitive_id < b->primitive_id;
 }
 
-/* trace_world, src/renderer/transport.h:43-85 */
-int or_trace_world(const or_view *s, const pt_ray *r, float low, float high, pt_flat_hit *hit,
-                   int brute, int tie_lowest, int *error, int *boxes, int *primitives) {
+/* trace_world, src/renderer/transport.h:43-85.  *ties (may be NULL) receives how many other
+ * primitives were hit at exactly the final closest distance: a primitive at that distance is
+ * tested whatever the visiting order, because boxes stay eligible up to nextafterf(closest). */
+static int trace_world_ties(const or_view *s, const pt_ray *r, float low, float high, pt_flat_hit *hit,
+                            int brute, int tie_lowest, int *error, int *boxes, int *primitives, int *ties) {
+    int same = 0;
+    if (ties) *ties = 0;
     if (s->root < 0) return 0;
     int found = 0;
     float closest = high;
@@ -209,10 +213,12 @@ int or_trace_world(const or_view *s, const pt_ray *r, float low, float high, pt_
             (*primitives)++;
             pt_flat_hit candidate;
             if (trace_leaf(s, n, r, low, high, &candidate) && (!found || candidate.t <= closest)) {
+                same = found && candidate.t == closest ? same + 1 : 0;
                 if (tie_lowest && found && candidate.t == closest && !lower_key(&candidate, hit)) continue;
                 *hit = candidate; closest = candidate.t; found = 1;
             }
         }
+        if (ties) *ties = found ? same : 0;
         return found;
     }
     int stack[OR_STACK], count = 0;
@@ -232,12 +238,19 @@ int or_trace_world(const or_view *s, const pt_ray *r, float low, float high, pt_
             pt_flat_hit candidate;
             float limit = found ? nextafterf(closest, high) : high;
             if (trace_leaf(s, n, r, low, limit, &candidate) && (!found || candidate.t <= closest)) {
+                same = found && candidate.t == closest ? same + 1 : 0;
                 if (tie_lowest && found && candidate.t == closest && !lower_key(&candidate, hit)) continue;
                 *hit = candidate; closest = candidate.t; found = 1;
             }
         }
     }
+    if (ties) *ties = found ? same : 0;
     return found;
+}
+
+int or_trace_world(const or_view *s, const pt_ray *r, float low, float high, pt_flat_hit *hit,
+                   int brute, int tie_lowest, int *error, int *boxes, int *primitives) {
+    return trace_world_ties(s, r, low, high, hit, brute, tie_lowest, error, boxes, primitives, NULL);
 }
 
 /* ------------------------------------------------------------------ threading helper */
@@ -263,15 +276,17 @@ static void parallel_for(size_t count, int threads, or_range_fn fn, void *ctx) {
 /* ------------------------------------------------------------------ batch queries */
 typedef struct {
     const or_view *s; const pt_ray *rays; int mode; float tmin; const float *tmax;
-    int brute, tie_lowest; pt_hit *hits; pt_ray_stats *stats;
+    int brute, tie_lowest; pt_hit *hits; pt_ray_stats *stats; int32_t *ties;
 } query_ctx;
 static void query_range(void *p, size_t b, size_t e) {
     query_ctx *q = (query_ctx *)p;
     for (size_t i = b; i < e; i++) {
         pt_flat_hit rec; memset(&rec, 0, sizeof rec);
-        int error = 0, boxes = 0, prims = 0;
+        int error = 0, boxes = 0, prims = 0, ties = 0;
         float hi = q->tmax ? q->tmax[i] : FLT_MAX;
-        int hit = or_trace_world(q->s, &q->rays[i], q->tmin, hi, &rec, q->brute, q->tie_lowest, &error, &boxes, &prims);
+        int hit = trace_world_ties(q->s, &q->rays[i], q->tmin, hi, &rec, q->brute, q->tie_lowest, &error, &boxes, &prims,
+                                   &ties);
+        if (q->ties) q->ties[i] = ties;
         pt_hit h;
         h.t = hit ? rec.t : 0.0f;
         h.primitive_id = hit ? rec.primitive_id : -1;
@@ -282,10 +297,15 @@ static void query_range(void *p, size_t b, size_t e) {
         if (q->stats) { q->stats[i].boxes = (uint32_t)boxes; q->stats[i].primitives = (uint32_t)prims; }
     }
 }
+void or_query_ties(const or_view *s, const pt_ray *rays, size_t count, int mode, float tmin,
+                   const float *tmax, int brute, int tie_lowest, pt_hit *hits, pt_ray_stats *stats,
+                   int32_t *ties, int threads) {
+    query_ctx q = {s, rays, mode, tmin, tmax, brute, tie_lowest, hits, stats, ties};
+    parallel_for(count, threads, query_range, &q);
+}
 void or_query(const or_view *s, const pt_ray *rays, size_t count, int mode, float tmin,
               const float *tmax, int brute, int tie_lowest, pt_hit *hits, pt_ray_stats *stats, int threads) {
-    query_ctx q = {s, rays, mode, tmin, tmax, brute, tie_lowest, hits, stats};
-    parallel_for(count, threads, query_range, &q);
+    or_query_ties(s, rays, count, mode, tmin, tmax, brute, tie_lowest, hits, stats, NULL, threads);
 }
 
 typedef struct { const or_view *s; const pt_ray *rays; int brute; pt_trace_result *out; } compat_ctx;

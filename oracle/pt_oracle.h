@@ -65,6 +65,11 @@ int or_trace_world(const or_view *s, const pt_ray *r, float low, float high, pt_
 void or_query(const or_view *s, const pt_ray *rays, size_t count, int mode, float tmin,
               const float *tmax, int brute, int tie_lowest, pt_hit *hits, pt_ray_stats *stats,
               int threads);
+/* or_query that also writes, per ray, how many other primitives were hit at exactly the
+ * closest distance (0 on a miss): ties[i] > 0 marks a ray whose answer a tie rule decides. */
+void or_query_ties(const or_view *s, const pt_ray *rays, size_t count, int mode, float tmin,
+                   const float *tmax, int brute, int tie_lowest, pt_hit *hits, pt_ray_stats *stats,
+                   int32_t *ties, int threads);
 /* cuda_query_rays semantics (src/cuda/cuda_renderer.cu:111-120) on the host. */
 void or_query_compat(const or_view *s, const pt_ray *rays, size_t count, int brute,
                      pt_trace_result *out, int threads);

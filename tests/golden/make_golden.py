@@ -11,6 +11,7 @@ the oracle without the reference present.
 """
 from __future__ import annotations
 
+import os
 import sys
 from pathlib import Path
 
@@ -24,7 +25,7 @@ sys.path.insert(0, str(ROOT / "oracle"))
 import ptb200 as pt  # noqa: E402
 from oracle_bind import RefCpu  # noqa: E402
 
-REF_ASSETS = Path("/root/reference/assets/models")
+REF_ASSETS = Path(os.environ.get("PT_REFERENCE_DIR", "/root/reference")) / "assets" / "models"
 
 
 def scene_arrays(prefix: str, s: pt.FlatScene) -> dict:

@@ -79,3 +79,17 @@ def test_batch_rejects_bad_jobs():
         pt.Batch(scenes, [bad])
     with pytest.raises(ValueError):
         pt.Batch(scenes, [dict(jobs[0], samples=0)])
+
+
+@pytest.mark.parametrize("fail_at", [1, 5])
+def test_autotune_skips_a_failed_probe_and_keeps_sample_counts(fail_at):
+    """A probe run that fails (injected on the host as a timed-out run) skips its setting; the
+    sweep goes on, and afterwards every job renders its full sample count."""
+    scenes, jobs = make_jobs()
+    b = pt.Batch(scenes, jobs)
+    pt.check(pt.library().pt_batch_fail_probe(b._h, fail_at))
+    best = b.autotune(probe_samples=1, cache_path=None)
+    assert best[1] in (128, 256)
+    b.run()
+    for k, j in enumerate(jobs):
+        assert b.sums(k).tobytes() == alone(scenes, j)[0].tobytes(), f"job {k}"

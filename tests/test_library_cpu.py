@@ -7,6 +7,7 @@ from __future__ import annotations
 
 import ctypes as C
 import re
+import sys
 from pathlib import Path
 
 import numpy as np
@@ -16,6 +17,7 @@ import ptb200 as pt
 from oracle_bind import Oracle, RefCpu, REF_CPU_SO, ORACLE_SO
 
 ROOT = Path(__file__).resolve().parents[1]
+sys.path.insert(0, str(ROOT))
 G = np.load(Path(__file__).parent / "golden" / "reference_golden.npz")
 
 
@@ -166,3 +168,20 @@ def test_oracle_lowest_id_tie_rule():
     assert st["primitives"][0] == 2 and stb["primitives"][0] == 3
     low = o.query(s, ray, tie_lowest=True)
     assert low["primitive_id"][0] == 0
+    # the tie counter sees both coincident spheres at t = 2 (one other primitive at that distance)
+    hits, ties = o.query_ties(s, ray)
+    assert hits.tobytes() == low.tobytes() and ties[0] == 1
+    ray2 = ray.copy()
+    ray2[0]["origin"] = (0.5, 0.5, -4)           # reaches only the far sphere: no tie
+    assert o.query_ties(s, ray2)[1][0] == 0
+
+
+def test_bench_samples_and_launch_counts():
+    """bench.py's seeded random subsets and its count of kernels per query call."""
+    import bench
+    a = bench.random_indices(1 << 20, 1000, 7)
+    assert len(a) == 1000 and len(np.unique(a)) == 1000 and (np.diff(a.astype(np.int64)) > 0).all()
+    assert np.array_equal(a, bench.random_indices(1 << 20, 1000, 7)) and a.max() < (1 << 20)
+    assert bench.walk_launches_per_query(1 << 25) == 8 and bench.walk_launches_per_query(1000) == 1
+    args = bench.parse([])
+    assert args.steps >= 1 and args.warmup >= 3 and args.parity_rays == 1 << 20 and args.log2_rays == 25

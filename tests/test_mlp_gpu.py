@@ -125,3 +125,42 @@ def test_weight_average_is_what_queries_use():
     torch.cuda.synchronize()
     got = out.cpu().numpy().reshape(n, 3)
     assert (np.abs(got - live) / np.maximum(np.abs(live), 1e-6)).max() < 2e-2
+
+
+def test_tensor_core_wait_timeout_is_reported_and_recoverable():
+    """Failure detection of the tensor-core kernels without a GPU fault: with a limit of 0 try_wait
+    attempts every bounded mbarrier wait runs out at once.  The forward pass and a training step
+    then report PT_TIMEOUT, the weights stay as they were (no Adam step is applied), each kernel
+    frees its TMEM after waiting for its own MMAs, and with the default limit back the same cache
+    answers exactly as before."""
+    torch = pytest.importorskip("torch")
+    cache = pt.RadianceCache(LO, HI, seed=3)
+    n = 4096
+    q = queries(n, 11)
+    t = target_fn(q)
+    qd, td = to_dev(q), to_dev(t)
+    out0 = torch.zeros(n * 3, dtype=torch.float32, device="cuda")
+    cache.query(qd, n, out0)
+    cache.sync()
+    l0, g0 = cache.gradients(qd, td, n)
+    w0 = cache.weights()
+    cache.wait_limit(0)
+    out1 = torch.full((n * 3,), -1.0, dtype=torch.float32, device="cuda")
+    cache.query(qd, n, out1)
+    with pytest.raises(pt.PtError) as e:
+        cache.sync()
+    assert e.value.status == 6                       # PT_TIMEOUT
+    with pytest.raises(pt.PtError) as e:
+        cache.train(qd, td, n, wait=True)
+    assert e.value.status == 6
+    assert np.array_equal(cache.weights(), w0)       # no step on a timed-out gradient pass
+    cache.wait_limit(-1)
+    cache.sync()                                     # nothing left pending
+    out2 = torch.zeros(n * 3, dtype=torch.float32, device="cuda")
+    cache.query(qd, n, out2)
+    cache.sync()
+    assert torch.equal(out0, out2)
+    l2, g2 = cache.gradients(qd, td, n)
+    assert np.array_equal(g0, g2) and l0 == l2
+    cache.train(qd, td, n, wait=True)
+    assert not np.array_equal(cache.weights(), w0)

@@ -12,7 +12,7 @@ import numpy as np
 import pytest
 
 import ptb200 as pt
-from oracle_bind import Oracle, RefGpu, REF_GPU_SO
+from oracle_bind import Oracle, RefCpu, RefGpu, REF_CPU_SO, REF_GPU_SO
 
 pytestmark = pytest.mark.gpu
 G = np.load(Path(__file__).parent / "golden" / "reference_golden.npz")
@@ -228,6 +228,80 @@ def test_ray_order_keeps_answers(oracle, layout):
     assert_hits_equal(got[pick], oracle.query(s, host[pick]))
 
 
+def _sample_rows(dev_u8, idx, width, dtype):
+    import torch
+    return dev_u8.view(-1, width)[torch.from_numpy(idx.astype(np.int64)).cuda()].cpu().numpy().view(dtype).reshape(-1)
+
+
+@pytest.mark.skipif(not REF_CPU_SO.exists(), reason="reference CPU build absent")
+def test_headline_scene_random_rays_vs_oracle_and_reference(oracle):
+    """The benchmark's own scene (1,048,580 triangles) and ray generators at full size: 2^24
+    camera rays and their 2^24 bounce rays walked in one 2^25-ray batch (key-ordered walk), and a
+    seeded random 2^18 of them compared with the oracle (type, id, t bitwise, lowest-id ties) and
+    with the reference's own trace_world wherever no exact-distance tie decides."""
+    torch = pytest.importorskip("torch")
+    s, cam = pt.procedural_scene(960, 600)
+    dev = pt.Scene(s)
+    half = 1 << 24
+    rays = torch.empty(2 * half * 28, dtype=torch.uint8, device="cuda")
+    hits = torch.empty(2 * half * 16, dtype=torch.uint8, device="cuda")
+    pt.camera_rays_device(cam, 960, 600, 1, 0, half, rays)
+    dev.query_device(rays, half, hits)
+    dev.bounce_rays_device(rays, hits, half, 2, 0, rays[half * 28:])
+    dev.query_device(rays, 2 * half, hits)
+    torch.cuda.synchronize()
+    idx = np.sort(np.random.default_rng(17).choice(2 * half, 1 << 18, replace=False))
+    r = _sample_rows(rays, idx, 28, pt.RAY)
+    got = _sample_rows(hits, idx, 16, pt.HIT)
+    del rays, hits
+    want, ties = oracle.query_ties(s, r)
+    assert_hits_equal(got, want)
+    res, _ = RefCpu().trace_world(s, r)
+    hit = res["hit"] == 1
+    assert np.array_equal(hit, got["primitive_type"] != 0)
+    no_tie = hit & (ties == 0)
+    assert np.array_equal(res["rec"]["primitive_id"][no_tie], got["primitive_id"][no_tie])
+    assert np.array_equal(res["rec"]["t"][hit].view(np.uint32), got["t"][hit].view(np.uint32))
+    assert (idx >= half).any() and (idx < half).any() and hit.mean() > 0.4
+
+
+@pytest.mark.skipif(not REF_CPU_SO.exists(), reason="reference CPU build absent")
+def test_microbenchmark_scene_closest_and_any_hit(oracle):
+    """The traversal microbenchmark's scene kind at reduced size (16 displaced spheres of 16,384
+    triangles and 65,536 random small triangles in a unit cube): camera rays and cosine surface
+    rays (closest hit) and shadow rays between surface points (any hit), generated on the device,
+    against the oracle and the reference's trace_world."""
+    torch = pytest.importorskip("torch")
+    s, cam = pt.procedural_scene(512, 512, sphere_count=16, segments=128, rings=65, box_size=1.0, radius_min=0.03,
+                                 radius_max=0.08, floor=0, light_fraction=0.0, random_triangles=1 << 16, seed=3)
+    dev = pt.Scene(s)
+    n = 1 << 18
+    rays = torch.empty(n * 28, dtype=torch.uint8, device="cuda")
+    pt.camera_rays_device(cam, 512, 512, 3, 0, n // 2, rays)
+    dev.surface_rays_device(4, 0, n // 2, rays[n // 2 * 28:])
+    hits = torch.empty(n * 16, dtype=torch.uint8, device="cuda")
+    dev.query_device(rays, n, hits)
+    host = rays.cpu().numpy().view(pt.RAY)
+    assert host[n // 2:].tobytes() == pt.surface_rays(s, 4, 0, n // 2).tobytes()
+    got = hits.cpu().numpy().view(pt.HIT)
+    pick = np.sort(np.random.default_rng(5).choice(n, 1 << 14, replace=False))
+    want, ties = oracle.query_ties(s, host[pick])
+    assert_hits_equal(got[pick], want)
+    tmax = torch.empty(n * 4, dtype=torch.uint8, device="cuda")
+    dev.surface_rays_device(5, 0, n, rays, tmax=tmax)
+    dev.query_device(rays, n, hits, mode=pt.QUERY_ANY, tmax=tmax)
+    host = rays.cpu().numpy().view(pt.RAY)
+    tm = tmax.cpu().numpy().view(np.float32)
+    sr, stm = pt.surface_rays(s, 5, 0, n, shadow=True)
+    assert host.tobytes() == sr.tobytes() and tm.tobytes() == stm.tobytes()
+    got = hits.cpu().numpy().view(pt.HIT)
+    want = oracle.query(s, host[pick], mode=pt.QUERY_ANY, tmax=tm[pick])
+    assert np.array_equal(got["primitive_type"][pick] != 0, want["primitive_id"] >= 0)
+    res, _ = RefCpu().trace_world(s, host[pick], tmax=tm[pick])
+    assert np.array_equal(got["primitive_type"][pick] != 0, res["hit"] == 1)
+    assert 0.05 < (got["primitive_type"] != 0).mean() < 0.95
+
+
 @pytest.mark.skipif(not REF_GPU_SO.exists(), reason="reference CUDA build absent")
 def test_matches_reference_gpu_query(layout):
     """Our compatibility query and the reference's own cuda_query_rays on the same B200."""
@@ -243,3 +317,70 @@ def test_invalid_scene_is_rejected():
     with pytest.raises(pt.PtError) as e:
         pt.Scene(s)
     assert e.value.status == 2
+
+
+def deepest_chain_scene(levels: int = 64):
+    """A tree of the greatest depth the reference's validator accepts (64 levels): every branch has
+    a branch on the left and one triangle leaf on the right, 64 stacked triangles, the nearest
+    (from below) at the bottom, so a ray along +z walks the whole chain."""
+    tris = np.zeros(levels, pt.TRIANGLE)
+    for k in range(levels):
+        z = 0.05 * k
+        tris[k]["v0"], tris[k]["v1"], tris[k]["v2"] = (-1, -1, z), (3, -1, z), (-1, 3, z)
+        tris[k]["n0"] = tris[k]["n1"] = tris[k]["n2"] = (0, 0, 1)
+    nodes = []
+
+    def box(ids):
+        lo = np.min([np.minimum(np.minimum(tris[i]["v0"], tris[i]["v1"]), tris[i]["v2"]) for i in ids], axis=0) - 1e-3
+        hi = np.max([np.maximum(np.maximum(tris[i]["v0"], tris[i]["v1"]), tris[i]["v2"]) for i in ids], axis=0) + 1e-3
+        return lo, hi
+
+    def build(level, ids):           # ids: triangles of this subtree, nearest first
+        me = len(nodes)
+        nodes.append(None)
+        lo, hi = box(ids)
+        if level == levels:
+            nodes[me] = (lo, hi, 1, -1, -1, ids[0])
+            return me
+        left = build(level + 1, ids[:-1])
+        right = len(nodes)
+        rlo, rhi = box(ids[-1:])
+        nodes.append((rlo, rhi, 1, -1, -1, ids[-1]))
+        nodes[me] = (lo, hi, 0, left, right, -1)
+        return me
+    build(1, list(range(levels)))
+    arr = np.zeros(len(nodes), pt.NODE)
+    for i, (lo, hi, t, l, r, p) in enumerate(nodes):
+        arr[i] = (lo, hi, t, l, r, p)
+    mats = np.zeros(1, pt.MATERIAL)
+    mats[0]["albedo"] = (0.5, 0.5, 0.5)
+    mats[0]["ref_idx"] = 1.0
+    tex = np.zeros(1, pt.TEXTURE)
+    tex[0]["color"] = (0.5, 0.5, 0.5)
+    return pt.FlatScene(tris, np.zeros(0, pt.SPHERE), arr, mats, tex, np.zeros(0, np.uint8), 0, levels)
+
+
+def test_deepest_valid_tree_matches_oracle_without_overflow(oracle, layout):
+    """trace_world's stack holds 64 entries and the validator bounds the depth at 64, which keeps
+    a validated tree from overflowing it (each level leaves at most one entry behind).  On the
+    deepest chain the reference accepts, the oracle reports no overflow (error 0), and every
+    traversal form gives the oracle's answers and error flags: closest hits from below and from
+    above, and any-hit shadow rays."""
+    s = deepest_chain_scene()
+    dev = pt.Scene(s)
+    g = np.random.default_rng(9)
+    n = 4096
+    rays = np.zeros(n, pt.RAY)
+    xy = g.uniform(-0.9, 0.9, (n, 2))
+    up = np.arange(n) % 2 == 0
+    rays["origin"] = np.c_[xy, np.where(up, -1.0, 4.0)]
+    rays["direction"] = np.c_[g.uniform(-0.05, 0.05, (n, 2)), np.where(up, 1.0, -1.0)]
+    want = oracle.query(s, rays)
+    assert not want["error"].any() and (want["primitive_type"] == 1).all()
+    assert_hits_equal(dev.query(rays), want)
+    assert set(np.unique(want["primitive_id"])) == {0, 63}
+    tmax = np.full(n, 1.5, np.float32)
+    got = dev.query(rays, mode=pt.QUERY_ANY, tmax=tmax)
+    want_any = oracle.query(s, rays, mode=pt.QUERY_ANY, tmax=tmax)
+    assert np.array_equal(got["primitive_type"] != 0, want_any["primitive_id"] >= 0)
+    assert not got["error"].any()
