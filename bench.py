@@ -924,6 +924,16 @@ def run_render(args):
     print(json.dumps(line), flush=True)
 
 
+def guarded(name, fn, *a, **k):
+    """Runs one sub-record; a failure is recorded in the line instead of ending the run."""
+    try:
+        return fn(*a, **k)
+    except Exception as e:  # noqa: BLE001 - the line reports what failed
+        import traceback
+        traceback.print_exc()
+        return {"error": f"{name}: {type(e).__name__}: {e}"}
+
+
 # --------------------------------------------------------------------------------------- headline
 def main(argv=None):
     args = parse(argv)
@@ -1028,7 +1038,7 @@ def main(argv=None):
                "sample": f"the parity sample ({len(sample_rays)} seeded random rays of the 2^25) x {passes} passes, "
                          f"trace_world on host_view, {total:.2f} s"}
         sub = np.arange(0, len(sample_rays), max(1, len(sample_rays) >> 18))
-        bvh = bvh_node_record(scene, sample_rays[sub], ref, threads, sample_hits[sub])
+        bvh = guarded("bvh_node", bvh_node_record, scene, sample_rays[sub], ref, threads, sample_hits[sub])
 
     # roofline of the walk kernel: algorithmic bytes from the reference's own box / primitive counts
     prof = profile_summary()
@@ -1047,7 +1057,7 @@ def main(argv=None):
 
     ref_gpu = None
     if extras and not args.no_ref_gpu:
-        ref_gpu = reference_gpu_record(scene, dev, rays, n, value)
+        ref_gpu = guarded("reference_gpu", reference_gpu_record, scene, dev, rays, n, value)
 
     launches = walk_launches_per_query(n)
     line = {
@@ -1068,12 +1078,12 @@ def main(argv=None):
     del rays, hits
     torch.cuda.empty_cache()
     if extras and not args.no_render:
-        line["render_c2"] = render_record(args, dev=dev, scene=scene, cam=cam)
+        line["render_c2"] = guarded("render_c2", render_record, args, dev=dev, scene=scene, cam=cam)
     dev.close()
     if extras and not args.no_c3:
-        line["c3"] = c3_record(args, hbm, l2_gbs, peak_kind)
+        line["c3"] = guarded("c3", c3_record, args, hbm, l2_gbs, peak_kind)
     if extras and not args.no_cache:
-        line["cache_c5"] = cache_record(args, diffuse_only=False, cpu=False)
+        line["cache_c5"] = guarded("cache_c5", cache_record, args, diffuse_only=False, cpu=False)
     if rank == 0:
         print(json.dumps(line), flush=True)
     ranks.close()
