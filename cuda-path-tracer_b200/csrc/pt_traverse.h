@@ -504,10 +504,57 @@ namespace ptb {
 
 // ---- four-wide traversal -------------------------------------------------------------------
 // Same answer as traverse<> (same primitive tests, same limit rule, same tie keys); fewer,
-// wider steps.  A step tests the four child boxes of a node with the reference's slab
-// arithmetic, visits the nearest passing child next and pushes the others, farthest first,
-// with their entry distance; a popped entry whose entry distance is no longer below the
-// current limit is dropped, which is exactly the box test repeated with the new limit.
+// wider steps.  A step tests the four child boxes of a node, visits the nearest passing child
+// next and pushes the others, farthest first, with their entry distance; a popped entry whose
+// entry distance is no longer below the current limit is dropped (the box test repeated with the
+// new limit).
+// The box tests only filter: a primitive the walk never reaches could change the answer only if
+// the ray hit it at a point outside a box around it, and every box holds its primitives' boxes,
+// which the reference pads by 1e-4 on every axis (src/geometry/triangle.h:96-109).  So the slab
+// values are computed in one fused multiply-add each, t = box * (1/d) + (-o * (1/d)), whose
+// rounding (a few ulps of t and of o/d) stays far inside that margin for scenes of up to a few
+// hundred units, and a box passes when entry <= exit.  A zero direction component is replaced
+// by +-1e-30 in the box test's inverse, so its slab accepts exactly the origins inside it.
+
+// Per-ray constants of the four-wide box test.
+struct RayBox4 {
+    float jx, jy, jz;      // 1/d per axis (|d| >= 1e-30)
+    float kx, ky, kz;      // -o * (1/d)
+    bool nx, ny, nz;       // 1/d < 0: the box's max plane is entered first
+};
+PT_HD inline RayBox4 ray_box4(const pt_ray &r) {
+    auto inv = [](float d) { return 1.0f / (fabsf(d) > 1e-30f ? d : (d < 0.0f ? -1e-30f : 1e-30f)); };
+    RayBox4 b;
+    b.jx = inv(r.direction.x); b.jy = inv(r.direction.y); b.jz = inv(r.direction.z);
+    b.kx = -(r.origin.x * b.jx); b.ky = -(r.origin.y * b.jy); b.kz = -(r.origin.z * b.jz);
+    b.nx = b.jx < 0; b.ny = b.jy < 0; b.nz = b.jz < 0;
+    return b;
+}
+PT_HD inline float fma_box(float a, float b, float c) {
+#ifdef __CUDA_ARCH__
+    return __fmaf_rn(a, b, c);
+#else
+    return std::fma(a, b, c);
+#endif
+}
+PT_HD inline float max3(float a, float b, float c) {
+#ifdef __CUDA_ARCH__
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+#else
+    return fmaxf(fmaxf(a, b), c);
+#endif
+}
+PT_HD inline float min3(float a, float b, float c) {
+#ifdef __CUDA_ARCH__
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+#else
+    return fminf(fminf(a, b), c);
+#endif
+}
 
 PT_HD inline void load_node4(const DeviceScene &s, int32_t node, Bvh4Node &n) {
 #ifdef __CUDA_ARCH__
@@ -527,18 +574,21 @@ PT_HD inline void load_node4(const DeviceScene &s, int32_t node, Bvh4Node &n) {
 }
 
 // Tests the children of `node`; returns how many passed, in `ref`/`dist` sorted nearest first.
-PT_HD inline int node4_children(const DeviceScene &s, int32_t node, const RayBox &rb, float tmin, float limit,
+PT_HD inline int node4_children(const DeviceScene &s, int32_t node, const RayBox4 &rb, float tmin, float limit,
                                 int32_t ref[4], float dist[4], uint32_t &boxes) {
     Bvh4Node n;
     load_node4(s, node, n);
     int hits = 0;
 #pragma unroll
     for (int k = 0; k < 4; k++) {
-        float e;
-        bool h = n.child[k] != kEmptyChild && box_hit(rb, n.lox[k], n.hix[k], n.loy[k], n.hiy[k], n.loz[k], n.hiz[k], tmin, limit, e);
+        const float ax = fma_box(rb.nx ? n.hix[k] : n.lox[k], rb.jx, rb.kx), bx = fma_box(rb.nx ? n.lox[k] : n.hix[k], rb.jx, rb.kx);
+        const float ay = fma_box(rb.ny ? n.hiy[k] : n.loy[k], rb.jy, rb.ky), by = fma_box(rb.ny ? n.loy[k] : n.hiy[k], rb.jy, rb.ky);
+        const float az = fma_box(rb.nz ? n.hiz[k] : n.loz[k], rb.jz, rb.kz), bz = fma_box(rb.nz ? n.loz[k] : n.hiz[k], rb.jz, rb.kz);
+        const float entry = fmaxf(max3(ax, ay, az), tmin), exit = fminf(min3(bx, by, bz), limit);
+        const bool h = n.child[k] != kEmptyChild && entry <= exit;
         boxes += n.child[k] != kEmptyChild;
         ref[k] = n.child[k];
-        dist[k] = h ? e : INFINITY;
+        dist[k] = h ? entry : INFINITY;
         hits += h;
     }
     // sorting network on (dist, ref), ascending
@@ -571,7 +621,7 @@ PT_HD inline bool traverse4_rt(const DeviceScene &s, const pt_ray &r, float tmin
                                HitInfo &hit, uint32_t &boxes, uint32_t &prims, int &error, int32_t root = 0) {
     hit.slot = -1; hit.t = 0; hit.u = 0; hit.v = 0;
     if (s.empty || s.node_count == 0 || root < 0) return false;
-    RayBox rb = ray_box(r);
+    RayBox4 rb = ray_box4(r);
     float dl = length(mk(r.direction));
     bool found = false;
     float closest = tmax, limit = tmax;
@@ -632,7 +682,7 @@ __device__ inline void persistent_walk4(const DeviceScene &s, size_t count, unsi
     int2 spill[kStack4 - kSharedStack4];
     const unsigned lane = threadIdx.x & 31;
     pt_ray r;
-    RayBox rb;
+    RayBox4 rb;
     float dl = 0, tmin = 0, tmax = 0, closest = 0, limit = 0;
     long long best_key = 0;
     HitInfo hit;
@@ -657,7 +707,7 @@ __device__ inline void persistent_walk4(const DeviceScene &s, size_t count, unsi
                 if (mine < count) {
                     index = mine;
                     get(index, r, tmin, tmax);
-                    rb = ray_box(r);
+                    rb = ray_box4(r);
                     dl = length(mk(r.direction));
                     closest = tmax; limit = tmax; best_key = 0;
                     hit.slot = -1; hit.t = 0; hit.u = 0; hit.v = 0;
@@ -739,7 +789,7 @@ __device__ inline void persistent_walk4_spec(const DeviceScene &s, size_t count,
     const unsigned lane = threadIdx.x & 31;
     constexpr int32_t kNone = kEmptyChild;
     pt_ray r;
-    RayBox rb;
+    RayBox4 rb;
     float dl = 0, tmin = 0, tmax = 0, closest = 0, limit = 0;
     long long best_key = 0;
     HitInfo hit;
@@ -774,7 +824,7 @@ __device__ inline void persistent_walk4_spec(const DeviceScene &s, size_t count,
                     int32_t root = 0;
                     if constexpr (kRoot) get(index, r, tmin, tmax, root);
                     else get(index, r, tmin, tmax);
-                    rb = ray_box(r);
+                    rb = ray_box4(r);
                     dl = length(mk(r.direction));
                     closest = tmax; limit = tmax; best_key = 0;
                     hit.slot = -1; hit.t = 0; hit.u = 0; hit.v = 0;
