@@ -231,8 +231,7 @@ void export_preorder(FlatScene &scene, const std::vector<BuildNode> &nodes, int3
     scene.root = 0;
 }
 
-void build_sah(FlatScene &scene, int threads) {
-    std::vector<BuildPrim> gathered = gather_prims(scene);
+std::vector<BuildNode> sah_tree(const std::vector<BuildPrim> &gathered, int threads, int32_t &root) {
     std::vector<Prim> prims;
     prims.reserve(gathered.size());
     for(const BuildPrim &g : gathered) {
@@ -242,7 +241,7 @@ void build_sah(FlatScene &scene, int threads) {
         prims.push_back(p);
     }
     Builder builder(prims, threads < 1 ? hardware_threads() : threads);
-    int32_t root = builder.run();
+    root = builder.run();
     std::vector<BuildNode> nodes(builder.nodes_.size());
     for(size_t i = 0; i < nodes.size(); i++) {
         const TNode &t = builder.nodes_[i];
@@ -250,6 +249,12 @@ void build_sah(FlatScene &scene, int threads) {
         for(int a = 0; a < 3; a++) { n.lo[a] = t.box.lo[a]; n.hi[a] = t.box.hi[a]; }
         n.left = t.left; n.right = t.right; n.type = t.type; n.prim = t.prim;
     }
+    return nodes;
+}
+
+void build_sah(FlatScene &scene, int threads) {
+    int32_t root = -1;
+    std::vector<BuildNode> nodes = sah_tree(gather_prims(scene), threads, root);
     export_preorder(scene, nodes, root);
 }
 

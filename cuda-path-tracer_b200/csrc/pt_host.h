@@ -61,6 +61,9 @@ struct BuildPrim { float lo[3], hi[3]; int32_t type, id; };
 struct BuildNode { float lo[3], hi[3]; int32_t left, right, type, prim; };
 std::vector<BuildPrim> gather_prims(const FlatScene &scene);
 void export_preorder(FlatScene &scene, const std::vector<BuildNode> &nodes, int32_t root);
+// Binned-SAH binary tree over arbitrary boxes (one per leaf; a leaf keeps its item's type and id);
+// `root` receives the root's index.  threads <= 0: all.
+std::vector<BuildNode> sah_tree(const std::vector<BuildPrim> &items, int threads, int32_t &root);
 // Linear BVH on the GPU (pt_lbvh.cu): Morton order of centroids, Karras's radix tree.
 void build_lbvh(FlatScene &scene);
 

@@ -1,17 +1,26 @@
-// pt_lbvh.cu — BVH construction on the GPU (linear BVH).
+// pt_lbvh.cu — BVH construction on the GPU (Morton order, agglomerative clustering, SAH top).
 //
 // Replaces the host build that produces the flattened arrays (the reference's bvh_node,
 // src/bvh/bvh.h:132-171, and this library's binned SAH, pt_build.cpp) for scenes that must be
-// built fast: primitives are ordered along a 63-bit Morton curve of their box centroids (21 bits
-// per axis over the centroid bounds), and the binary radix tree over the sorted codes is built
-// with every internal node in parallel (Karras, "Maximizing Parallelism in the Construction of
-// BVHs, Octrees, and k-d Trees", HPG 2012; equal codes are told apart by their sorted index).
-// Boxes are unions of the children's, computed bottom-up (a node's second arriving child
-// computes it), so every node box encloses the reference's padded primitive boxes exactly.
-// The tree is exported on the host with the same preorder as the SAH builder (one primitive per
-// leaf, depth <= 64).  Tree quality is that of a linear BVH: traversal is somewhat slower than
-// on the SAH tree; the build is much faster.
+// built fast.  Three stages:
+//   1. primitives are ordered along a 63-bit Morton curve of their box centroids (21 bits per
+//      axis over the centroid bounds; a radix sort on the device);
+//   2. locally-ordered clustering on the device (Meister and Bittner, "Parallel Locally-Ordered
+//      Clustering for Bounding Volume Hierarchy Construction", 2018): in every round each cluster
+//      finds, among the clusters up to kRadius places away in Morton order, the one whose union
+//      with it has the smallest surface area (ties: the lower index, so pairs are totally
+//      ordered and the best pair is always mutual); mutual nearest neighbours merge into a new
+//      node at the lower index, and the clusters are compacted in order.  Rounds run until a
+//      quarter of the primitives' count remains (each cluster then holds a few primitives);
+//   3. the binned-SAH builder of pt_build.cpp splits the remaining cluster boxes on the host, and
+//      the clusters' subtrees hang under its leaves.
+// Boxes are unions of the children's, so every node box encloses the reference's padded
+// primitive boxes exactly.  The tree is exported with the SAH builder's preorder (one primitive
+// per leaf, depth <= 64).  Merging by nearest neighbour makes the lowest levels a little worse
+// than SAH splits: the tree traverses a few percent slower than the host SAH tree.
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
+#include <cub/device/device_select.cuh>
 #include <algorithm>
 #include <cfloat>
 #include <vector>
@@ -76,72 +85,74 @@ __global__ void morton_codes(const BuildPrim *prims, int n, const unsigned int *
     order[i] = i;
 }
 
-// length of the common prefix of sorted keys i and j (index bits break ties); -1 outside
-__device__ inline int delta(const uint64_t *k, int n, int i, int j) {
-    if (j < 0 || j >= n) return -1;
-    uint64_t a = k[i], b = k[j];
-    if (a == b) return 64 + __clz(unsigned(i) ^ unsigned(j));
-    return __clzll(a ^ b);
+constexpr int kRadius = 16;         // neighbours searched on each side, in Morton order
+constexpr int kNearBlock = 256;
+
+__device__ inline float merged_area(const Bounds &a, const Bounds &b) {
+    float dx = fmaxf(a.hi[0], b.hi[0]) - fminf(a.lo[0], b.lo[0]);
+    float dy = fmaxf(a.hi[1], b.hi[1]) - fminf(a.lo[1], b.lo[1]);
+    float dz = fmaxf(a.hi[2], b.hi[2]) - fminf(a.lo[2], b.lo[2]);
+    return 2.0f * (dx * dy + dy * dz + dz * dx);
 }
 
-// Internal node i of n - 1: its key range, split and children.  Children are encoded as
-// internal index (>= 0) or ~leaf index (< 0).
-__global__ void radix_tree(const uint64_t *k, int n, int32_t *left, int32_t *right, int32_t *parent_internal,
-                           int32_t *parent_leaf) {
+// leaf k (k-th primitive in Morton order) is node k; every leaf starts as its own cluster
+__global__ void leaf_boxes(const BuildPrim *prims, const int32_t *order, int n, Bounds *boxes, int32_t *clusters) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const BuildPrim &p = prims[order[k]];
+    Bounds b;
+    for (int a = 0; a < 3; a++) { b.lo[a] = p.lo[a]; b.hi[a] = p.hi[a]; }
+    boxes[k] = b;
+    clusters[k] = k;
+}
+
+// nearest neighbour of every cluster within kRadius places (smallest merged area, then lowest index)
+__global__ void __launch_bounds__(kNearBlock) nearest(const Bounds *boxes, const int32_t *clusters, int count, int32_t *nn) {
+    __shared__ Bounds tile[kNearBlock + 2 * kRadius];
+    const int base = blockIdx.x * kNearBlock;
+    for (int t = threadIdx.x; t < kNearBlock + 2 * kRadius; t += kNearBlock) {
+        int j = base - kRadius + t;
+        if (j >= 0 && j < count) tile[t] = boxes[clusters[j]];
+    }
+    __syncthreads();
+    const int i = base + threadIdx.x;
+    if (i >= count) return;
+    const Bounds bi = tile[threadIdx.x + kRadius];
+    float best = FLT_MAX;
+    int32_t bj = -1;
+    for (int d = -kRadius; d <= kRadius; d++) {
+        const int j = i + d;
+        if (d == 0 || j < 0 || j >= count) continue;
+        const float area = merged_area(bi, tile[threadIdx.x + kRadius + d]);
+        if (area < best) { best = area; bj = j; }
+    }
+    nn[i] = bj;
+}
+
+// merge[i] = 1 when cluster i is the lower index of a mutual pair; keep[i] = 0 for the upper one
+__global__ void pair_flags(const int32_t *nn, int count, int32_t *merge, unsigned char *keep) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n - 1) return;
-    int d = delta(k, n, i, i + 1) - delta(k, n, i, i - 1) >= 0 ? 1 : -1;
-    int dmin = delta(k, n, i, i - d);
-    int lmax = 2;
-    while (delta(k, n, i, i + lmax * d) > dmin) lmax *= 2;
-    int l = 0;
-    for (int t = lmax / 2; t >= 1; t /= 2)
-        if (delta(k, n, i, i + (l + t) * d) > dmin) l += t;
-    int j = i + l * d;
-    int dnode = delta(k, n, i, j);
-    int s = 0;
-    for (int div = 2;; div *= 2) {
-        int t = (l + div - 1) / div;
-        if (delta(k, n, i, i + (s + t) * d) > dnode) s += t;
-        if (t == 1) break;
-    }
-    int g = i + s * d + min(d, 0);
-    int lo = min(i, j), hi = max(i, j);
-    int32_t lc = lo == g ? ~g : g;
-    int32_t rc = hi == g + 1 ? ~(g + 1) : g + 1;
-    left[i] = lc;
-    right[i] = rc;
-    if (lc < 0) parent_leaf[~lc] = i; else parent_internal[lc] = i;
-    if (rc < 0) parent_leaf[~rc] = i; else parent_internal[rc] = i;
+    if (i >= count) return;
+    const int32_t j = nn[i];
+    const bool mutual = j >= 0 && nn[j] == i;
+    merge[i] = mutual && i < j;
+    keep[i] = !(mutual && i > j);
 }
 
-// Bottom-up boxes: each leaf climbs; at every node the first arriving child stops, the second
-// unions both children's boxes and climbs on.
-__global__ void refit(const BuildPrim *prims, const int32_t *order, int n, const int32_t *left, const int32_t *right,
-                      const int32_t *parent_internal, const int32_t *parent_leaf, unsigned int *arrivals, Bounds *boxes) {
-    int leaf = blockIdx.x * blockDim.x + threadIdx.x;
-    if (leaf >= n) return;
-    int node = parent_leaf[leaf];
-    while (node >= 0) {
-        __threadfence();
-        if (atomicAdd(&arrivals[node], 1u) == 0) return;
-        __threadfence();
-        Bounds b;
-        for (int a = 0; a < 3; a++) { b.lo[a] = FLT_MAX; b.hi[a] = -FLT_MAX; }
-        const int32_t kids[2] = {left[node], right[node]};
-        for (int c = 0; c < 2; c++) {
-            int32_t kid = kids[c];
-            if (kid < 0) {
-                const BuildPrim &p = prims[order[~kid]];
-                for (int a = 0; a < 3; a++) { b.lo[a] = fminf(b.lo[a], p.lo[a]); b.hi[a] = fmaxf(b.hi[a], p.hi[a]); }
-            } else {
-                const volatile Bounds &q = boxes[kid];
-                for (int a = 0; a < 3; a++) { b.lo[a] = fminf(b.lo[a], q.lo[a]); b.hi[a] = fmaxf(b.hi[a], q.hi[a]); }
-            }
-        }
-        boxes[node] = b;
-        node = parent_internal[node];
-    }
+// the lower cluster of each mutual pair becomes a new node (numbered by the pairs' scan)
+__global__ void merge_pairs(const int32_t *clusters, const int32_t *nn, const int32_t *merge, const int32_t *slot, int count,
+                            int32_t node_base, Bounds *boxes, int32_t *left, int32_t *right, int32_t *merged) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    if (!merge[i]) { merged[i] = clusters[i]; return; }
+    const int32_t a = clusters[i], b = clusters[nn[i]], id = node_base + slot[i];
+    Bounds u;
+    const Bounds ba = boxes[a], bb = boxes[b];
+    for (int k = 0; k < 3; k++) { u.lo[k] = fminf(ba.lo[k], bb.lo[k]); u.hi[k] = fmaxf(ba.hi[k], bb.hi[k]); }
+    boxes[id] = u;
+    left[id] = a;
+    right[id] = b;
+    merged[i] = id;
 }
 
 } // namespace lbvh
@@ -162,53 +173,100 @@ void build_lbvh(FlatScene &scene) {
         return;
     }
     require_device();
-    DeviceBuffer d_prims, d_bounds, d_codes, d_codes_sorted, d_order, d_order_sorted, d_left, d_right, d_pi, d_pl, d_arr, d_boxes, d_temp;
+    // node ids: leaf k = k (Morton order), merged nodes from n upwards (at most n - 1 of them)
+    const size_t total = size_t(2 * n - 1);
+    DeviceBuffer d_prims, d_bounds, d_codes, d_codes_sorted, d_order, d_order_sorted, d_boxes, d_left, d_right, d_clusters,
+        d_merged, d_nn, d_merge, d_slot, d_keep, d_count, d_temp;
     d_prims.upload(prims);
     const unsigned int init[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
     d_bounds.upload(init, sizeof init);
     d_codes.resize(size_t(n) * 8); d_codes_sorted.resize(size_t(n) * 8);
     d_order.resize(size_t(n) * 4); d_order_sorted.resize(size_t(n) * 4);
-    d_left.resize(size_t(n - 1) * 4); d_right.resize(size_t(n - 1) * 4);
-    d_pi.resize(size_t(n - 1) * 4); d_pl.resize(size_t(n) * 4);
-    d_arr.resize(size_t(n - 1) * 4); d_boxes.resize(size_t(n - 1) * sizeof(Bounds));
-    PT_CUDA(cudaMemset(d_arr.get(), 0, size_t(n - 1) * 4));
-    PT_CUDA(cudaMemset(d_pi.get(), 0xff, size_t(n - 1) * 4));    // root's parent = -1
+    d_boxes.resize(total * sizeof(Bounds));
+    d_left.resize(total * 4); d_right.resize(total * 4);
+    d_clusters.resize(size_t(n) * 4); d_merged.resize(size_t(n) * 4); d_nn.resize(size_t(n) * 4);
+    d_merge.resize(size_t(n) * 4); d_slot.resize(size_t(n) * 4); d_keep.resize(size_t(n)); d_count.resize(2 * sizeof(int32_t));
     const int blocks = (n + 255) / 256;
     centroid_bounds<<<blocks, 256>>>(d_prims.get<BuildPrim>(), n, d_bounds.get<unsigned int>());
     morton_codes<<<blocks, 256>>>(d_prims.get<BuildPrim>(), n, d_bounds.get<unsigned int>(), d_codes.get<uint64_t>(), d_order.get<int32_t>());
     PT_CUDA(cudaGetLastError());
-    size_t temp = 0;
-    PT_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, temp, d_codes.get<uint64_t>(), d_codes_sorted.get<uint64_t>(),
+    size_t sort_temp = 0, scan_temp = 0, select_temp = 0;
+    PT_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, sort_temp, d_codes.get<uint64_t>(), d_codes_sorted.get<uint64_t>(),
                                             d_order.get<int32_t>(), d_order_sorted.get<int32_t>(), n, 0, 63));
-    d_temp.resize(std::max<size_t>(temp, 1));
-    PT_CUDA(cub::DeviceRadixSort::SortPairs(d_temp.get(), temp, d_codes.get<uint64_t>(), d_codes_sorted.get<uint64_t>(),
+    PT_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, scan_temp, d_merge.get<int32_t>(), d_slot.get<int32_t>(), n));
+    PT_CUDA(cub::DeviceSelect::Flagged(nullptr, select_temp, d_merged.get<int32_t>(), d_keep.get<unsigned char>(),
+                                       d_clusters.get<int32_t>(), d_count.get<int32_t>(), n));
+    d_temp.resize(std::max<size_t>({sort_temp, scan_temp, select_temp, 1}));
+    PT_CUDA(cub::DeviceRadixSort::SortPairs(d_temp.get(), sort_temp, d_codes.get<uint64_t>(), d_codes_sorted.get<uint64_t>(),
                                             d_order.get<int32_t>(), d_order_sorted.get<int32_t>(), n, 0, 63));
-    radix_tree<<<(n - 1 + 255) / 256, 256>>>(d_codes_sorted.get<uint64_t>(), n, d_left.get<int32_t>(), d_right.get<int32_t>(),
-                                              d_pi.get<int32_t>(), d_pl.get<int32_t>());
-    refit<<<blocks, 256>>>(d_prims.get<BuildPrim>(), d_order_sorted.get<int32_t>(), n, d_left.get<int32_t>(), d_right.get<int32_t>(),
-                           d_pi.get<int32_t>(), d_pl.get<int32_t>(), d_arr.get<unsigned int>(), d_boxes.get<Bounds>());
+    leaf_boxes<<<blocks, 256>>>(d_prims.get<BuildPrim>(), d_order_sorted.get<int32_t>(), n, d_boxes.get<Bounds>(),
+                                d_clusters.get<int32_t>());
     PT_CUDA(cudaGetLastError());
-    std::vector<int32_t> left(size_t(n - 1)), right(size_t(n - 1)), order(static_cast<size_t>(n));
-    std::vector<Bounds> boxes(size_t(n - 1));
-    PT_CUDA(cudaMemcpy(left.data(), d_left.get(), left.size() * 4, cudaMemcpyDeviceToHost));
-    PT_CUDA(cudaMemcpy(right.data(), d_right.get(), right.size() * 4, cudaMemcpyDeviceToHost));
-    PT_CUDA(cudaMemcpy(order.data(), d_order_sorted.get(), order.size() * 4, cudaMemcpyDeviceToHost));
-    PT_CUDA(cudaMemcpy(boxes.data(), d_boxes.get(), boxes.size() * sizeof(Bounds), cudaMemcpyDeviceToHost));
-    // nodes: internal 0..n-2, then leaf k at n-1+k
-    std::vector<BuildNode> nodes(size_t(2 * n - 1));
-    auto child = [&](int32_t c) { return c < 0 ? int32_t(n - 1 + ~c) : c; };
-    for (int i = 0; i < n - 1; i++) {
-        BuildNode &b = nodes[size_t(i)];
-        for (int a = 0; a < 3; a++) { b.lo[a] = boxes[size_t(i)].lo[a]; b.hi[a] = boxes[size_t(i)].hi[a]; }
-        b.left = child(left[size_t(i)]); b.right = child(right[size_t(i)]); b.type = PT_BRANCH; b.prim = -1;
+    // clustering rounds until a quarter of the primitives' count remains
+    const int stop = std::max(1, n / 4);
+    int count = n;
+    int32_t next = n;
+    for (int round = 0; count > stop; round++) {
+        if (round > 4 * n) throw Error(PT_INVALID_ARGUMENT, "clustering did not converge");
+        const int cb = (count + 255) / 256;
+        nearest<<<(count + kNearBlock - 1) / kNearBlock, kNearBlock>>>(d_boxes.get<Bounds>(), d_clusters.get<int32_t>(), count,
+                                                                     d_nn.get<int32_t>());
+        pair_flags<<<cb, 256>>>(d_nn.get<int32_t>(), count, d_merge.get<int32_t>(), d_keep.get<unsigned char>());
+        PT_CUDA(cudaGetLastError());
+        PT_CUDA(cub::DeviceScan::ExclusiveSum(d_temp.get(), scan_temp, d_merge.get<int32_t>(), d_slot.get<int32_t>(), count));
+        merge_pairs<<<cb, 256>>>(d_clusters.get<int32_t>(), d_nn.get<int32_t>(), d_merge.get<int32_t>(), d_slot.get<int32_t>(), count,
+                                 next, d_boxes.get<Bounds>(), d_left.get<int32_t>(), d_right.get<int32_t>(), d_merged.get<int32_t>());
+        PT_CUDA(cudaGetLastError());
+        PT_CUDA(cub::DeviceSelect::Flagged(d_temp.get(), select_temp, d_merged.get<int32_t>(), d_keep.get<unsigned char>(),
+                                           d_clusters.get<int32_t>(), d_count.get<int32_t>(), count));
+        int32_t remaining = 0;
+        PT_CUDA(cudaMemcpy(&remaining, d_count.get(), sizeof remaining, cudaMemcpyDeviceToHost));
+        next += count - remaining;     // one new node per merged pair
+        count = remaining;
     }
+    std::vector<int32_t> left(total, -1), right(total, -1), clusters(static_cast<size_t>(count)), order(static_cast<size_t>(n));
+    std::vector<Bounds> boxes(total);
+    PT_CUDA(cudaMemcpy(left.data() + n, d_left.get<int32_t>() + n, size_t(next - n) * 4, cudaMemcpyDeviceToHost));
+    PT_CUDA(cudaMemcpy(right.data() + n, d_right.get<int32_t>() + n, size_t(next - n) * 4, cudaMemcpyDeviceToHost));
+    PT_CUDA(cudaMemcpy(boxes.data(), d_boxes.get(), size_t(next) * sizeof(Bounds), cudaMemcpyDeviceToHost));
+    PT_CUDA(cudaMemcpy(clusters.data(), d_clusters.get(), size_t(count) * 4, cudaMemcpyDeviceToHost));
+    PT_CUDA(cudaMemcpy(order.data(), d_order_sorted.get(), order.size() * 4, cudaMemcpyDeviceToHost));
+    std::vector<BuildNode> nodes(total);
     for (int k = 0; k < n; k++) {
         const BuildPrim &p = prims[size_t(order[size_t(k)])];
-        BuildNode &b = nodes[size_t(n - 1 + k)];
+        BuildNode &b = nodes[size_t(k)];
         for (int a = 0; a < 3; a++) { b.lo[a] = p.lo[a]; b.hi[a] = p.hi[a]; }
         b.left = b.right = -1; b.type = p.type; b.prim = p.id;
     }
-    export_preorder(scene, nodes, 0);
+    for (int32_t id = n; id < next; id++) {
+        BuildNode &b = nodes[size_t(id)];
+        for (int a = 0; a < 3; a++) { b.lo[a] = boxes[size_t(id)].lo[a]; b.hi[a] = boxes[size_t(id)].hi[a]; }
+        b.left = left[size_t(id)]; b.right = right[size_t(id)]; b.type = PT_BRANCH; b.prim = -1;
+    }
+    int32_t root = clusters[0];
+    if (count > 1) {
+        // binned SAH over the remaining clusters' boxes; the clusters hang under its leaves
+        std::vector<BuildPrim> items(static_cast<size_t>(count));
+        for (int i = 0; i < count; i++) {
+            const BuildNode &c = nodes[size_t(clusters[size_t(i)])];
+            for (int a = 0; a < 3; a++) { items[size_t(i)].lo[a] = c.lo[a]; items[size_t(i)].hi[a] = c.hi[a]; }
+            items[size_t(i)].type = PT_TRIANGLE;
+            items[size_t(i)].id = clusters[size_t(i)];
+        }
+        int32_t top_root = -1;
+        std::vector<BuildNode> top = sah_tree(items, 0, top_root);
+        std::vector<int32_t> id_of(top.size());
+        for (size_t k = 0; k < top.size(); k++) id_of[k] = top[k].type == PT_BRANCH ? next++ : top[k].prim;
+        for (size_t k = 0; k < top.size(); k++) {
+            if (top[k].type != PT_BRANCH) continue;
+            BuildNode &b = nodes[size_t(id_of[k])];
+            b = top[k];
+            b.left = id_of[size_t(top[k].left)];
+            b.right = id_of[size_t(top[k].right)];
+        }
+        root = id_of[size_t(top_root)];
+    }
+    export_preorder(scene, nodes, root);
 }
 
 } // namespace ptb
