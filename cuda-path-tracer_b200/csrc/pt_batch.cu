@@ -30,10 +30,10 @@ struct BatchJob {
     int32_t width, height, samples, max_depth;
     uint64_t seed;
     int64_t pixel_offset;
-    int32_t pixel_count, root;
+    int32_t pixel_count, root;        // root: the job's tree in the four-wide node array (-1: empty)
     int32_t light_offset, light_count;
     float light_area;
-    int32_t pad;
+    int32_t root2;                    // the job's tree in the two-wide node array (-1: empty)
 };
 
 struct BatchBuffers {
@@ -130,7 +130,8 @@ __global__ void batch_start(BatchBuffers b, int32_t slots) {
     b.queue[0][k] = k;
 }
 
-template <bool kSpec>
+// kWide: four-wide nodes (phased walk) or the two-wide layout.
+template <bool kWide>
 __global__ void batch_extend(DeviceScene scene, BatchBuffers b, int parity, int min_active) {
     const int32_t n = b.counters[parity];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -144,7 +145,8 @@ __global__ void batch_extend(DeviceScene scene, BatchBuffers b, int parity, int 
         int32_t slot = queue[k];
         r = path_ray(b.paths[slot]);
         lo = 0.001f; hi = FLT_MAX;
-        root = b.jobs[b.slot_job[slot]].root;
+        const BatchJob &j = b.jobs[b.slot_job[slot]];
+        root = kWide ? j.root : j.root2;
     };
     auto done = [&](size_t k, const WalkResult &w) {
         if (w.error) *b.error = 1;
@@ -152,7 +154,8 @@ __global__ void batch_extend(DeviceScene scene, BatchBuffers b, int parity, int 
         out.t = w.t; out.u = w.u; out.v = w.v; out.slot = w.error ? -2 : w.slot;
         b.hits[queue[k]] = out;
     };
-    persistent_walk4_spec<false, true>(scene, size_t(n), &b.fetch[0], min_active, kTieLastLeaf, get, done);
+    if constexpr (kWide) persistent_walk4_spec<false, true>(scene, size_t(n), &b.fetch[0], min_active, kTieLastLeaf, get, done);
+    else persistent_walk<false, true>(scene, size_t(n), &b.fetch[0], min_active, kTieLastLeaf, get, done);
 }
 
 __global__ void batch_shade(DeviceScene scene, BatchBuffers b, int parity) {
@@ -202,6 +205,7 @@ __global__ void batch_shade(DeviceScene scene, BatchBuffers b, int parity) {
     }
 }
 
+template <bool kWide>
 __global__ void batch_shadow(DeviceScene scene, BatchBuffers b, int parity, int min_active) {
     const int32_t n = b.counters[2 + parity];
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(b.rays, (unsigned long long)n);
@@ -212,7 +216,8 @@ __global__ void batch_shadow(DeviceScene scene, BatchBuffers b, int parity, int 
         r.direction = pt_vec3{sr.dx, sr.dy, sr.dz};
         r.time = sr.time;
         lo = 0.001f; hi = sr.tmax;
-        root = b.jobs[b.slot_job[slot]].root;
+        const BatchJob &j = b.jobs[b.slot_job[slot]];
+        root = kWide ? j.root : j.root2;
     };
     auto done = [&](size_t k, const WalkResult &w) {
         if (w.error) { *b.error = 1; return; }
@@ -223,7 +228,8 @@ __global__ void batch_shadow(DeviceScene scene, BatchBuffers b, int parity, int 
             s.rr = s.rr + sr.cr; s.rg = s.rg + sr.cg; s.rb = s.rb + sr.cb;
         }
     };
-    persistent_walk4_spec<true, true>(scene, size_t(n), &b.fetch[1 + parity], min_active, kTieLastLeaf, get, done);
+    if constexpr (kWide) persistent_walk4_spec<true, true>(scene, size_t(n), &b.fetch[1 + parity], min_active, kTieLastLeaf, get, done);
+    else persistent_walk<true, true>(scene, size_t(n), &b.fetch[1 + parity], min_active, kTieLastLeaf, get, done);
 }
 
 // One thread: continue the WHILE loop while paths are live, unless only a short tail is left
@@ -240,10 +246,11 @@ __global__ void batch_control(BatchBuffers b, cudaGraphConditionalHandle handle,
 
 // The tail, two lanes per slot: in each round the even lane of a pair walks its path's next ray
 // while the odd lane walks the shadow ray of the path's previous bounce (one runtime-mode walk,
-// traverse4_rt), so a bounce costs one walk's latency instead of two.  The shadow contribution of
+// traverse4_rt or traverse_rt), so a bounce costs one walk's latency instead of two.  The shadow contribution of
 // bounce k is added before bounce k+1 is shaded, the order of the iterations above, so the sums
 // are bit-identical.  A pair whose pixel is done takes the next pixel while any remain, then the next
 // queued slot (fetch[3]).
+template <bool kWide>
 __global__ void __launch_bounds__(256, 2) batch_finish_pair(DeviceScene scene, BatchBuffers b) {
     const int32_t n = b.counters[0];
     const unsigned full = 0xffffffffu;
@@ -292,15 +299,19 @@ __global__ void __launch_bounds__(256, 2) batch_finish_pair(DeviceScene scene, B
         }
         const bool work = odd ? walk_shadow : live;   // both lanes' rounds stay in step (warp-uniform loop)
         if (!__any_sync(full, work)) break;
-        const int32_t root = odd ? qroot : (live ? b.jobs[jid].root : 0);
+        const int32_t root = odd ? qroot : (live ? (kWide ? b.jobs[jid].root : b.jobs[jid].root2) : 0);
         HitInfo hi;
         uint32_t boxes = 0, prims = 0;
         int error = 0;
         bool hit = false;
         if (work) {
             rays++;
-            hit = traverse4_rt(scene, odd ? q : path_ray(s), 0.001f, odd ? qmax : FLT_MAX, kTieLastLeaf, odd, hi, boxes, prims,
-                               error, root);
+            if constexpr (kWide)
+                hit = traverse4_rt(scene, odd ? q : path_ray(s), 0.001f, odd ? qmax : FLT_MAX, kTieLastLeaf, odd, hi, boxes, prims,
+                                   error, root);
+            else
+                hit = traverse_rt(scene, odd ? q : path_ray(s), 0.001f, odd ? qmax : FLT_MAX, kTieLastLeaf, odd, hi, boxes, prims,
+                                  error, root);
         }
         const bool blocked = __shfl_sync(full, hit, odd_lane);
         const int shadow_error = __shfl_sync(full, error, odd_lane);
@@ -353,7 +364,7 @@ struct PinnedWords {
 
 struct pt_batch {
     DeviceScene view{};
-    DeviceBuffer nodes4, tris, spheres, triangles, sphere_src, materials, textures, pixels, lights, jobs;
+    DeviceBuffer nodes4, nodes2, tris, spheres, triangles, sphere_src, materials, textures, pixels, lights, jobs;
     DeviceBuffer sums, rng, paths, hits, shadows, slot_pixel, slot_job, queue0, queue1, shadow_queue, counters, fetch, scalars,
         job_remaining, job_done_ns, error;
     std::vector<BatchJob> host_jobs;
@@ -362,6 +373,7 @@ struct pt_batch {
     int mis = 1;
     // tuning (pt_batch_tuning / pt_batch_autotune)
     int32_t capacity = 0, block = 256, min_active = 16, tail_paths = 16384, use_graph = 1;
+    int32_t wide = 1;                     // node fetch width: 1 four-wide nodes, 0 the two-wide layout
     int32_t probe_fault_countdown = 0;   // > 0: that autotune probe run fails on the host (tests)
     int32_t slots = 0;
     BatchBuffers buf{};
@@ -385,7 +397,16 @@ struct pt_batch {
         if (graph) cudaGraphDestroy(graph);
         exec = nullptr; graph = nullptr;
     }
-    size_t stack_smem() const { return size_t(kSharedStack4) * sizeof(int2) * size_t(block); }
+    size_t stack_smem() const {
+        return wide ? size_t(kSharedStack4) * sizeof(int2) * size_t(block) : size_t(kSharedStack) * sizeof(int32_t) * size_t(block);
+    }
+    const void *extend_fn() const { return wide ? (const void *)batch_extend<true> : (const void *)batch_extend<false>; }
+    const void *shadow_fn() const { return wide ? (const void *)batch_shadow<true> : (const void *)batch_shadow<false>; }
+    const void *finish_fn() const { return wide ? (const void *)batch_finish_pair<true> : (const void *)batch_finish_pair<false>; }
+    void launch_finish(cudaStream_t st) {
+        if (wide) batch_finish_pair<true><<<grid(finish_fn(), 0), block, 0, st>>>(view, buf);
+        else batch_finish_pair<false><<<grid(finish_fn(), 0), block, 0, st>>>(view, buf);
+    }
     int grid(const void *fn, size_t smem) const {
         int per_sm = 0;
         PT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, smem));
@@ -416,12 +437,14 @@ struct pt_batch {
     void pair(cudaStream_t st) {
         const size_t smem = stack_smem();
         for (int parity = 0; parity < 2; parity++) {
-            batch_extend<true><<<grid((const void *)batch_extend<true>, smem), block, smem, st>>>(view, buf, parity, min_active);
+            if (wide) batch_extend<true><<<grid(extend_fn(), smem), block, smem, st>>>(view, buf, parity, min_active);
+            else batch_extend<false><<<grid(extend_fn(), smem), block, smem, st>>>(view, buf, parity, min_active);
             if (parity == 1) PT_CUDA(cudaStreamWaitEvent(st, shadowed[0].get(), 0));
             batch_shade<<<grid((const void *)batch_shade, 0), block, 0, st>>>(view, buf, parity);
             PT_CUDA(cudaEventRecord(shaded[parity].get(), st));
             PT_CUDA(cudaStreamWaitEvent(shadow_stream, shaded[parity].get(), 0));
-            batch_shadow<<<grid((const void *)batch_shadow, smem), block, smem, shadow_stream>>>(view, buf, parity, min_active);
+            if (wide) batch_shadow<true><<<grid(shadow_fn(), smem), block, smem, shadow_stream>>>(view, buf, parity, min_active);
+            else batch_shadow<false><<<grid(shadow_fn(), smem), block, smem, shadow_stream>>>(view, buf, parity, min_active);
             PT_CUDA(cudaEventRecord(shadowed[parity].get(), shadow_stream));
         }
         PT_CUDA(cudaStreamWaitEvent(st, shadowed[1].get(), 0));
@@ -445,7 +468,7 @@ struct pt_batch {
         batch_control<<<1, 32, 0, stream>>>(buf, handle, tail_paths, max_iterations());
         PT_CUDA(cudaStreamEndCapture(stream, &body));
         PT_CUDA(cudaStreamBeginCaptureToGraph(stream, graph, &loop, nullptr, 1, cudaStreamCaptureModeRelaxed));
-        batch_finish_pair<<<grid((const void *)batch_finish_pair, 0), block, 0, stream>>>(view, buf);
+        launch_finish(stream);
         PT_CUDA(cudaStreamEndCapture(stream, &graph));
         PT_CUDA(cudaGraphInstantiate(&exec, graph, 0));
     }
@@ -479,7 +502,7 @@ struct pt_batch {
                 if (live == 0 || (live < tail_paths && cursor >= (unsigned long long)total_pixels)) break;
                 if (it + 1 >= bound) throw Error(PT_TIMEOUT, "batch did not drain within its iteration bound");
             }
-            batch_finish_pair<<<grid((const void *)batch_finish_pair, 0), block, 0, st>>>(view, buf);
+            launch_finish(st);
         }
         PT_CUDA(cudaGetLastError());
         PT_CUDA(cudaEventRecord(stop.get(), st));
@@ -503,7 +526,7 @@ struct pt_batch {
 namespace {
 // Merges every scene's host layout into one: four-wide nodes, slots, primitives, materials,
 // textures, pixels and emitter tables, with their indices offset.
-void merge_scenes(pt_batch *b, const pt_scene_desc *descs, int32_t count, std::vector<int32_t> &roots,
+void merge_scenes(pt_batch *b, const pt_scene_desc *descs, int32_t count, std::vector<int32_t> &roots, std::vector<int32_t> &roots2,
                   std::vector<int32_t> &light_offset, std::vector<int32_t> &light_count, std::vector<float> &light_area) {
     std::vector<HostLayout> layouts(static_cast<size_t>(count));
     int64_t total_tri_slots = 0;
@@ -515,6 +538,7 @@ void merge_scenes(pt_batch *b, const pt_scene_desc *descs, int32_t count, std::v
         total_tri_slots += int64_t(layouts[size_t(i)].tris.size());
     }
     std::vector<Bvh4Node> nodes4;
+    std::vector<BvhNode> nodes2;
     std::vector<TriRecord> tris;
     std::vector<SphereRecord> spheres;
     std::vector<pt_triangle> triangles;
@@ -527,7 +551,7 @@ void merge_scenes(pt_batch *b, const pt_scene_desc *descs, int32_t count, std::v
     for (int32_t i = 0; i < count; i++) {
         const pt_scene_desc &d = descs[i];
         HostLayout &L = layouts[size_t(i)];
-        const int32_t node_base = int32_t(nodes4.size());
+        const int32_t node_base = int32_t(nodes4.size()), node2_base = int32_t(nodes2.size());
         const int64_t tri_slot_base = int64_t(tris.size());
         const int32_t local_tri_slots = int32_t(L.tris.size());
         const int32_t tri_base = int32_t(triangles.size()), sphere_base = int32_t(sphere_src.size());
@@ -536,6 +560,22 @@ void merge_scenes(pt_batch *b, const pt_scene_desc *descs, int32_t count, std::v
         if (total_tri_slots + sphere_slot_base + int64_t(L.spheres.size()) >= (int64_t(1) << 28))
             throw Error(PT_INVALID_ARGUMENT, "batched scenes exceed 2^28 primitives");
         roots.push_back(d.root < 0 ? -1 : node_base);
+        roots2.push_back(d.root < 0 ? -1 : node2_base);
+        // a two-wide leaf reference is ~slot of one primitive
+        auto slot2 = [&](int32_t c) -> int32_t {
+            if (c == kEmptyChild) return c;
+            if (c >= 0) return c + node2_base;
+            const int32_t k = ~c;
+            const int64_t g = k < local_tri_slots ? tri_slot_base + k : total_tri_slots + sphere_slot_base + (k - local_tri_slots);
+            return ~int32_t(g);
+        };
+        if (d.root >= 0) {
+            for (BvhNode n : L.nodes) {
+                n.child0 = slot2(n.child0);
+                n.child1 = slot2(n.child1);
+                nodes2.push_back(n);
+            }
+        }
         for (Bvh4Node n : L.nodes4) {
             for (int k = 0; k < 4; k++) {
                 int32_t c = n.child[k];
@@ -575,11 +615,11 @@ void merge_scenes(pt_batch *b, const pt_scene_desc *descs, int32_t count, std::v
         for (pt_light l : own) { l.primitive += l.type == PT_TRIANGLE ? tri_base : sphere_base; lights.push_back(l); }
     }
     b->total_triangles = triangles.size();
-    b->nodes4.upload(nodes4); b->tris.upload(tris); b->spheres.upload(spheres); b->triangles.upload(triangles);
+    b->nodes4.upload(nodes4); b->nodes2.upload(nodes2); b->tris.upload(tris); b->spheres.upload(spheres); b->triangles.upload(triangles);
     b->sphere_src.upload(sphere_src); b->materials.upload(materials); b->textures.upload(textures);
     b->pixels.upload(pixels.data(), pixels.size()); b->lights.upload(lights);
     DeviceScene &v = b->view;
-    v.nodes = nullptr;
+    v.nodes = nodes2.empty() ? nullptr : b->nodes2.get<BvhNode>();
     v.nodes4 = nodes4.empty() ? nullptr : b->nodes4.get<Bvh4Node>();
     v.tris = b->tris.get<TriRecord>(); v.spheres = b->spheres.get<SphereRecord>();
     v.triangles = b->triangles.get<pt_triangle>(); v.sphere_src = b->sphere_src.get<pt_sphere>();
@@ -611,16 +651,16 @@ pt_status pt_batch_create(const pt_scene_desc *scenes, int32_t scene_count, cons
         require_device();
         auto b = new pt_batch;
         try {
-            std::vector<int32_t> roots, loff, lcount;
+            std::vector<int32_t> roots, roots2, loff, lcount;
             std::vector<float> larea;
-            merge_scenes(b, scenes, scene_count, roots, loff, lcount, larea);
+            merge_scenes(b, scenes, scene_count, roots, roots2, loff, lcount, larea);
             int64_t offset = 0;
             for (int32_t k = 0; k < job_count; k++) {
                 const pt_job &j = jobs[k];
                 BatchJob bj{};
                 bj.camera = j.camera; bj.width = j.width; bj.height = j.height; bj.samples = j.samples; bj.max_depth = j.max_depth;
                 bj.seed = j.seed; bj.pixel_offset = offset; bj.pixel_count = j.width * j.height;
-                bj.root = roots[size_t(j.scene)]; bj.light_offset = loff[size_t(j.scene)]; bj.light_count = lcount[size_t(j.scene)];
+                bj.root = roots[size_t(j.scene)]; bj.root2 = roots2[size_t(j.scene)]; bj.light_offset = loff[size_t(j.scene)]; bj.light_count = lcount[size_t(j.scene)];
                 bj.light_area = larea[size_t(j.scene)];
                 offset += bj.pixel_count;
                 b->host_jobs.push_back(bj);
@@ -668,6 +708,15 @@ pt_status pt_batch_tuning(pt_batch *b, int32_t path_capacity, int32_t block, int
     });
 }
 
+// Node fetch width of the batch's walks: 1 = four-wide nodes, 0 = the two-wide layout.
+pt_status pt_batch_node_width(pt_batch *b, int32_t wide) {
+    return guard([&]() {
+        if (!b) throw Error(PT_INVALID_ARGUMENT, "null batch");
+        if ((wide ? 1 : 0) != b->wide) b->drop_graph();
+        b->wide = wide ? 1 : 0;
+    });
+}
+
 pt_status pt_batch_run(pt_batch *b) {
     return guard([&]() {
         if (!b) throw Error(PT_INVALID_ARGUMENT, "null batch");
@@ -703,16 +752,17 @@ pt_status pt_batch_fail_probe(pt_batch *b, int32_t n) {
 }
 
 // Autotuner: times probe runs (every job at min(probe_samples, its samples)) over path-pool
-// capacity, block size, refill threshold and graph/host loop, keeps the fastest, and caches it per
-// (log2 triangles, log2 pixels) bucket in a text file (one "bucket capacity block min_active
-// use_graph ms" line per bucket).  With a cached entry for the bucket the sweep is skipped.
+// capacity, block size, refill threshold and graph/host loop, then the other node fetch width at
+// the fastest of those, keeps the fastest, and caches it per (log2 triangles, log2 pixels) bucket
+// in a text file (one "bucket capacity block min_active use_graph node_width ms" line per bucket).
+// With a cached entry for the bucket the sweep is skipped.
 pt_status pt_batch_autotune(pt_batch *b, int32_t probe_samples, const char *cache_path, int32_t *best) {
     return guard([&]() {
         if (!b || probe_samples <= 0) throw Error(PT_INVALID_ARGUMENT, "invalid autotune arguments");
         int tb = int(std::log2(double(std::max<uint64_t>(1, b->total_triangles))));
         int pb = int(std::log2(double(std::max<int64_t>(1, b->total_pixels))));
         std::string bucket = "tri" + std::to_string(tb) + "_px" + std::to_string(pb);
-        int32_t cfg[4] = {0, 256, 16, 1};
+        int32_t cfg[5] = {0, 256, 16, 1, 1};
         bool cached = false;
         std::vector<std::string> lines;
         if (cache_path) {
@@ -722,8 +772,10 @@ pt_status pt_batch_autotune(pt_batch *b, int32_t probe_samples, const char *cach
                 lines.push_back(line);
                 std::istringstream ss(line);
                 std::string key;
-                int32_t c0, c1, c2, c3;
-                if (ss >> key >> c0 >> c1 >> c2 >> c3 && key == bucket) { cfg[0] = c0; cfg[1] = c1; cfg[2] = c2; cfg[3] = c3; cached = true; }
+                int32_t c0, c1, c2, c3, c4;
+                if (ss >> key >> c0 >> c1 >> c2 >> c3 >> c4 && key == bucket) {
+                    cfg[0] = c0; cfg[1] = c1; cfg[2] = c2; cfg[3] = c3; cfg[4] = c4; cached = true;
+                }
             }
         }
         if (!cached) {
@@ -736,6 +788,7 @@ pt_status pt_batch_autotune(pt_batch *b, int32_t probe_samples, const char *cach
                     try { b->jobs.upload(b->host_jobs); } catch (...) {}
                 }
             } restore{b, b->host_jobs};
+            if (!b->wide) { b->wide = 1; b->drop_graph(); }   // the sweep runs on four-wide nodes
             for (auto &j : b->host_jobs) j.samples = std::min(j.samples, probe_samples);
             b->jobs.upload(b->host_jobs);
             const int32_t caps[] = {1 << 20, 1 << 21, 1 << 22};
@@ -758,14 +811,26 @@ pt_status pt_batch_autotune(pt_batch *b, int32_t probe_samples, const char *cach
                 if (b->milliseconds < best_ms) { best_ms = b->milliseconds; cfg[0] = cap; cfg[1] = blk; cfg[2] = act; cfg[3] = graph; }
             }
             if (best_ms == 1e30) throw Error(PT_INVALID_ARGUMENT, "every autotune setting failed: " + failure);
+            // node fetch width at the best setting: the four-wide nodes against the two-wide layout
+            for (int32_t w : {0, 1}) {
+                if (w == cfg[4]) continue;
+                if (pt_batch_tuning(b, cfg[0], cfg[1], cfg[2], b->tail_paths, cfg[3]) != PT_OK) continue;
+                b->wide = w;
+                b->drop_graph();
+                try { b->run(); } catch (const Error &e) { if (e.status == PT_CUDA_ERROR) throw; continue; }
+                if (b->milliseconds < best_ms) { best_ms = b->milliseconds; cfg[4] = w; }
+            }
+            b->wide = cfg[4];
+            b->drop_graph();
             if (cache_path) {
                 std::ofstream outf(cache_path, std::ios::app);
-                outf << bucket << " " << cfg[0] << " " << cfg[1] << " " << cfg[2] << " " << cfg[3] << " " << best_ms << "\n";
+                outf << bucket << " " << cfg[0] << " " << cfg[1] << " " << cfg[2] << " " << cfg[3] << " " << cfg[4] << " " << best_ms << "\n";
             }
         }
         pt_status st = pt_batch_tuning(b, cfg[0], cfg[1], cfg[2], b->tail_paths, cfg[3]);
         if (st != PT_OK) throw Error(st, pt_last_error());
-        if (best) { best[0] = cfg[0]; best[1] = cfg[1]; best[2] = cfg[2]; best[3] = cfg[3]; }
+        if ((cfg[4] ? 1 : 0) != b->wide) { b->wide = cfg[4] ? 1 : 0; b->drop_graph(); }
+        if (best) { best[0] = cfg[0]; best[1] = cfg[1]; best[2] = cfg[2]; best[3] = cfg[3]; best[4] = cfg[4]; }
     });
 }
 

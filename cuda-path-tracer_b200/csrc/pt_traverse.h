@@ -105,12 +105,12 @@ PT_HD __forceinline__ bool test_leaf(const DeviceScene &s, int32_t slot, const p
     return test_leaf_rt(s, slot, r, dl, tmin, tmax, tie, kAny, found, closest, best_key, hit, prims);
 }
 
-// Closest hit (kAny = false) or any hit (kAny = true) over (tmin, tmax).
-template <bool kAny>
-PT_HD inline bool traverse(const DeviceScene &s, const pt_ray &r, float tmin, float tmax, int tie,
-                           HitInfo &hit, uint32_t &boxes, uint32_t &prims, int &error) {
+// Closest hit (any = false) or any hit (any = true) over (tmin, tmax), from node `root` of the
+// two-wide array (several trees may share it).
+PT_HD inline bool traverse_rt(const DeviceScene &s, const pt_ray &r, float tmin, float tmax, int tie, bool any,
+                              HitInfo &hit, uint32_t &boxes, uint32_t &prims, int &error, int32_t root = 0) {
     hit.slot = -1; hit.t = 0; hit.u = 0; hit.v = 0;
-    if (s.empty || s.node_count == 0) return false;
+    if (s.empty || s.node_count == 0 || root < 0) return false;
     RayBox rb = ray_box(r);
     float dl = length(mk(r.direction));
     bool found = false;
@@ -118,7 +118,7 @@ PT_HD inline bool traverse(const DeviceScene &s, const pt_ray &r, float tmin, fl
     long long best_key = 0;
     int32_t stack[kStackCapacity];
     int sp = 0;
-    int32_t node = 0;
+    int32_t node = root;
     for (;;) {
         BvhNode n;
         load_node(s, node, n);
@@ -138,12 +138,12 @@ PT_HD inline bool traverse(const DeviceScene &s, const pt_ray &r, float tmin, fl
         int ninner = 0;
         if (hf) {
             if (first < 0) {
-                if (test_leaf<kAny>(s, ~first, r, dl, tmin, tmax, tie, found, closest, best_key, hit, prims) && kAny) return true;
+                if (test_leaf_rt(s, ~first, r, dl, tmin, tmax, tie, any, found, closest, best_key, hit, prims) && any) return true;
             } else inner[ninner++] = first;
         }
         if (hs) {
             if (second < 0) {
-                if (test_leaf<kAny>(s, ~second, r, dl, tmin, tmax, tie, found, closest, best_key, hit, prims) && kAny) return true;
+                if (test_leaf_rt(s, ~second, r, dl, tmin, tmax, tie, any, found, closest, best_key, hit, prims) && any) return true;
             } else inner[ninner++] = second;
         }
         if (ninner == 2) {
@@ -158,6 +158,11 @@ PT_HD inline bool traverse(const DeviceScene &s, const pt_ray &r, float tmin, fl
         }
     }
     return found;
+}
+template <bool kAny>
+PT_HD inline bool traverse(const DeviceScene &s, const pt_ray &r, float tmin, float tmax, int tie,
+                           HitInfo &hit, uint32_t &boxes, uint32_t &prims, int &error) {
+    return traverse_rt(s, r, tmin, tmax, tie, kAny, hit, boxes, prims, error, 0);
 }
 
 // trace_world in the reference's own visiting order (src/renderer/transport.h:61-84): a
@@ -385,8 +390,9 @@ struct WalkResult { float t, u, v; int32_t slot; uint32_t boxes, prims; int erro
 // atomicAdd per warp); between traversal steps a warp hands new items to idle lanes once fewer
 // than `min_active` lanes are busy.  get(k, ray, tmin, tmax) loads item k; done(k, result)
 // consumes a finished walk.  Every lane of the warp must call this together, and the block
-// must provide kSharedStack * blockDim.x int32 words of dynamic shared memory.
-template <bool kAny, class Get, class Done>
+// must provide kSharedStack * blockDim.x int32 words of dynamic shared memory.  With kRoot, get()
+// also returns the walk's root node (several trees in one node array; < 0 for an empty tree).
+template <bool kAny, bool kRoot = false, class Get, class Done>
 __device__ inline void persistent_walk(const DeviceScene &s, size_t count, unsigned long long *next, int min_active,
                                        int tie, Get get, Done done) {
     // Warps past the first `count` lanes have nothing to take: they leave before touching the
@@ -423,13 +429,15 @@ __device__ inline void persistent_walk(const DeviceScene &s, size_t count, unsig
                 size_t mine = base + __popc(idle & ((1u << lane) - 1u));
                 if (mine < count) {
                     index = mine;
-                    get(index, r, tmin, tmax);
+                    int32_t root = 0;
+                    if constexpr (kRoot) get(index, r, tmin, tmax, root);
+                    else get(index, r, tmin, tmax);
                     rb = ray_box(r);
                     dl = length(mk(r.direction));
                     closest = tmax; best_key = 0;
                     hit.slot = -1; hit.t = 0; hit.u = 0; hit.v = 0;
                     boxes = 0; prims = 0; sp = 0; found = false; error = 0;
-                    node = (s.empty || s.node_count == 0) ? -1 : 0;
+                    node = (s.empty || s.node_count == 0 || root < 0) ? -1 : root;
                     busy = true;
                 }
             }

@@ -160,6 +160,7 @@ def library() -> C.CDLL:
         "pt_batch_tuning": (I, [P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
         "pt_batch_autotune": (I, [P, C.c_int32, C.c_char_p, P]),
         "pt_batch_fail_probe": (I, [P, C.c_int32]),
+        "pt_batch_node_width": (I, [P, C.c_int32]),
         "pt_cache_create": (I, [P, P, U64, P]),
         "pt_cache_destroy": (I, [P]),
         "pt_cache_query_device": (I, [P, P, S, P, P]),
@@ -656,8 +657,13 @@ class Batch:
     def tuning(self, path_capacity=0, block=256, min_active=16, tail_paths=16384, use_graph=1) -> None:
         check(library().pt_batch_tuning(self._h, path_capacity, block, min_active, tail_paths, use_graph))
 
+    def node_width(self, wide: int) -> None:
+        """Four-wide nodes (1) or the two-wide layout (0) for the batch's walks (pt_batch_node_width)."""
+        check(library().pt_batch_node_width(self._h, int(wide)))
+
     def autotune(self, probe_samples: int = 1, cache_path: str | None = None):
-        best = (C.c_int32 * 4)()
+        """(capacity, block, min_active, use_graph, node_width) of the fastest probe run (pt_batch_autotune)."""
+        best = (C.c_int32 * 5)()
         check(library().pt_batch_autotune(self._h, probe_samples, cache_path.encode() if cache_path else None, best))
         return tuple(best)
 

@@ -271,9 +271,13 @@ pt_status pt_batch_stats(const pt_batch *batch, float *kernel_ms, uint64_t *rays
  * use_graph: 1 = one graph launch with a device-side loop, 0 = host-driven loop. */
 pt_status pt_batch_tuning(pt_batch *batch, int32_t path_capacity, int32_t block, int32_t min_active, int32_t tail_paths,
                           int32_t use_graph);
+/* Node fetch width of the batch's walks: 1 = four-wide nodes (default), 0 = the two-wide layout.
+ * Results do not depend on it. */
+pt_status pt_batch_node_width(pt_batch *batch, int32_t wide);
 /* Sweeps capacity x block x min_active x graph on probe runs (each job at min(probe_samples, its
- * samples)), applies the fastest and caches it per (log2 triangles, log2 pixels) bucket in
- * `cache_path` (NULL: no cache).  best = {capacity, block, min_active, use_graph}.  A probe run that
+ * samples)), then the other node fetch width at the fastest of those, applies the fastest and caches
+ * it per (log2 triangles, log2 pixels) bucket in `cache_path` (NULL: no cache).  best (5 entries) =
+ * {capacity, block, min_active, use_graph, node_width}.  A probe run that
  * fails (timeout, stack overflow) skips its setting; the jobs' sample counts are restored whatever
  * happens; a CUDA error ends the sweep with PT_CUDA_ERROR. */
 pt_status pt_batch_autotune(pt_batch *batch, int32_t probe_samples, const char *cache_path, int32_t *best);

@@ -28,12 +28,14 @@ def alone(scenes, job, mis=True):
     return r.sums(), r.rays_traced()
 
 
+@pytest.mark.parametrize("wide", [1, 0], ids=["four-wide", "two-wide"])
 @pytest.mark.parametrize("graph", [1, 0], ids=["graph", "host-loop"])
 @pytest.mark.parametrize("capacity", [0, 700], ids=["all-slots", "small-pool"])
-def test_batch_matches_lone_renderers(graph, capacity):
+def test_batch_matches_lone_renderers(graph, capacity, wide):
     scenes, jobs = make_jobs()
     b = pt.Batch(scenes, jobs)
     b.tuning(path_capacity=capacity, use_graph=graph)
+    b.node_width(wide)
     b.run()
     ms, rays, done = b.stats()
     total = 0
@@ -89,7 +91,7 @@ def test_autotune_skips_a_failed_probe_and_keeps_sample_counts(fail_at):
     b = pt.Batch(scenes, jobs)
     pt.check(pt.library().pt_batch_fail_probe(b._h, fail_at))
     best = b.autotune(probe_samples=1, cache_path=None)
-    assert best[1] in (128, 256)
+    assert best[1] in (128, 256) and best[4] in (0, 1)
     b.run()
     for k, j in enumerate(jobs):
         assert b.sums(k).tobytes() == alone(scenes, j)[0].tobytes(), f"job {k}"
