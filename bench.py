@@ -71,6 +71,8 @@ def parse(argv=None):
     ap.add_argument("--no-ref-gpu", action="store_true")
     ap.add_argument("--parity-rays", type=int, default=1 << 20)
     ap.add_argument("--c3-log2-rays", type=int, default=25)
+    ap.add_argument("--dump-rays", default=None,
+                    help="directory: write the 2^24 camera and 2^24 bounce rays as raw 28-byte records (the reference's ray layout)")
     ap.add_argument("--workload", choices=["query", "batch48", "cache", "mlp", "render", "c3"], default="query",
                     help="query: the closest-hit benchmark with its sub-records (default); batch48: 48 render jobs in "
                          "one launch; cache: radiance-cache renderer vs plain at 1920x1080; render: config-2 renderer "
@@ -841,13 +843,14 @@ def run_cache(args):
 
 
 # --------------------------------------------------------------------------------------- config 2 render
-def render_record(args, dev=None, scene=None, cam=None, steps: int = 3, warmup: int = 1, cpu: bool = False):
-    """The progressive renderer on the procedural 1M-triangle scene, 960x600, 64 spp, bounce limit
-    8, MIS (one step = a full 64-spp render from a reset), beside the reference's own CUDA
-    renderer built with its bounce limit set to 8 ("patched reference", oracle/_ref) on the same
+def render_record(args, dev=None, scene=None, cam=None, steps: int = 3, warmup: int = 1, cpu: bool = False,
+                  W: int = 960, H: int = 600, SPP: int = 64, D: int = 8,
+                  workload: str = "progressive render of the procedural 1M-triangle scene, 960x600, 64 spp, bounce limit 8, MIS"):
+    """The progressive renderer (one step = a full render from a reset; by default the procedural
+    1M-triangle scene, 960x600, 64 spp, bounce limit 8, MIS) beside the reference's own CUDA
+    renderer built with its bounce limit set to D ("patched reference", oracle/_ref) on the same
     GPU: Mrays/s = rays traced / kernel time, as the reference reports it
     (src/cuda/cuda_renderer.cu:196-213, 246-247), and the two images compared bitwise."""
-    W, H, SPP, D = 960, 600, 64, 8
     t = time.perf_counter()
     if dev is None:
         scene, cam = pt.procedural_scene(W, H)
@@ -900,9 +903,9 @@ def render_record(args, dev=None, scene=None, cam=None, steps: int = 3, warmup: 
         cpu_rec = {"value": crays / dt / 1e6, "unit": "Mrays/s", "cores": threads, "kind": "reference",
                    "sample": f"reference trace_pixel_sample (bounce limit 50) on the same scene, {W}x{H} x {SPP} spp: "
                              f"{crays} rays in {dt:.2f} s"}
-    return {"workload": "progressive render of the procedural 1M-triangle scene, 960x600, 64 spp, bounce limit 8, MIS",
+    return {"workload": workload,
             "mrays_per_s": value, "ms_per_render": ms / steps, "rays_per_render": rays / steps, "steps": steps,
-            "reference_gpu": ref_line, "target": ">= 3x the reference renderer's Mrays/s with identical images",
+            "reference_gpu": ref_line, "target": ">= 3x the reference renderer's Mrays/s with identical images" if W == 960 else None,
             "e2e_mrays_per_s": rays / wall / 1e6, "scene_build_s": build_s, "cpu_baseline": cpu_rec}
 
 
@@ -967,6 +970,12 @@ def main(argv=None):
     dev.query_device(rays, n_each, hits)
     dev.bounce_rays_device(rays, hits, n_each, 2, 0, rays[n_each * 28:])
     torch.cuda.synchronize()
+
+    if args.dump_rays and rank == 0:
+        d = Path(args.dump_rays)
+        d.mkdir(parents=True, exist_ok=True)
+        rays[:n_each * 28].cpu().numpy().tofile(d / "config2_camera_2^24.ray")
+        rays[n_each * 28:].cpu().numpy().tofile(d / "config2_bounce_2^24.ray")
 
     # the timed region: K closest-hit passes over the 2^25 rays (legacy default stream)
     clocks = Clocks(local)
@@ -1079,6 +1088,10 @@ def main(argv=None):
     torch.cuda.empty_cache()
     if extras and not args.no_render:
         line["render_c2"] = guarded("render_c2", render_record, args, dev=dev, scene=scene, cam=cam)
+        cornell, ccam = pt.cornell_box(320, 200)
+        line["render_c1"] = guarded("render_c1", render_record, args, dev=pt.Scene(cornell), scene=cornell, cam=ccam, steps=5,
+                                    warmup=2, W=320, H=200, SPP=16, D=8, cpu=True,
+                                    workload="Cornell box (20 triangles, 3 spheres), 320x200, 16 spp, bounce limit 8, MIS, seed 1")
     dev.close()
     if extras and not args.no_c3:
         line["c3"] = guarded("c3", c3_record, args, hbm, l2_gbs, peak_kind)

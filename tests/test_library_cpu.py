@@ -185,3 +185,16 @@ def test_bench_samples_and_launch_counts():
     assert bench.walk_launches_per_query(1 << 25) == 8 and bench.walk_launches_per_query(1000) == 1
     args = bench.parse([])
     assert args.steps >= 1 and args.warmup >= 3 and args.parity_rays == 1 << 20 and args.log2_rays == 25
+
+
+def test_ray_records_are_the_reference_ray_layout(tmp_path):
+    """Ray dumps (bench.py --dump-rays) are raw records of the reference's ray (src/core/ray.h:30-32:
+    origin vec3, direction vec3, time float = 28 bytes); written and read back unchanged."""
+    assert pt.RAY.itemsize == 28
+    assert [pt.RAY.fields[k][1] for k in ("origin", "direction", "time")] == [0, 12, 24]
+    s, cam = pt.cornell_box(32, 20)
+    rays = pt.camera_rays(cam, 32, 20, 1, 0, 1000)
+    f = tmp_path / "camera.ray"
+    rays.view(np.uint8).tofile(f)
+    assert f.stat().st_size == 28 * 1000
+    assert np.fromfile(f, dtype=pt.RAY).tobytes() == rays.tobytes()
