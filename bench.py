@@ -914,7 +914,7 @@ def run_render(args):
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     clocks = Clocks(local)
-    rec = render_record(args, steps=max(1, args.steps), warmup=max(1, args.warmup), cpu=True)
+    rec = render_record(args, steps=max(1, args.steps), warmup=max(1, args.warmup), cpu=not args.no_cpu_baseline)
     clock = clocks.stop()
     line = {"metric": "Mrays/s render (procedural 1M, 960x600, 64 spp, depth 8, MIS)", "value": rec["mrays_per_s"],
             "unit": "Mrays/s", "n_gpus": 1, "steps": rec["steps"], "warmup": max(1, args.warmup),
