@@ -564,17 +564,29 @@ PT_HD inline float min3(float a, float b, float c) {
 #endif
 }
 
+#ifdef __CUDA_ARCH__
+// eight consecutive words of a 32-byte aligned address, one 256-bit load through the read-only path
+__device__ __forceinline__ void ldg8(const float *p, float (&v)[8]) {
+    asm volatile("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]), "=f"(v[7])
+                 : "l"(p));
+}
+#endif
+
 PT_HD inline void load_node4(const DeviceScene &s, int32_t node, Bvh4Node &n) {
 #ifdef __CUDA_ARCH__
-    const float4 *p = reinterpret_cast<const float4 *>(&s.nodes4[node]);
-    float4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2), d = __ldg(p + 3), e = __ldg(p + 4), f = __ldg(p + 5);
-    int4 g = __ldg(reinterpret_cast<const int4 *>(p + 6));
-    n.lox[0] = a.x; n.lox[1] = a.y; n.lox[2] = a.z; n.lox[3] = a.w;
-    n.hix[0] = b.x; n.hix[1] = b.y; n.hix[2] = b.z; n.hix[3] = b.w;
-    n.loy[0] = c.x; n.loy[1] = c.y; n.loy[2] = c.z; n.loy[3] = c.w;
-    n.hiy[0] = d.x; n.hiy[1] = d.y; n.hiy[2] = d.z; n.hiy[3] = d.w;
-    n.loz[0] = e.x; n.loz[1] = e.y; n.loz[2] = e.z; n.loz[3] = e.w;
-    n.hiz[0] = f.x; n.hiz[1] = f.y; n.hiz[2] = f.z; n.hiz[3] = f.w;
+    const float *p = reinterpret_cast<const float *>(&s.nodes4[node]);   // 128-byte aligned
+    float x[8], y[8], z[8];
+    ldg8(p, x);
+    ldg8(p + 8, y);
+    ldg8(p + 16, z);
+    const int4 g = __ldg(reinterpret_cast<const int4 *>(p + 24));
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        n.lox[k] = x[k]; n.hix[k] = x[4 + k];
+        n.loy[k] = y[k]; n.hiy[k] = y[4 + k];
+        n.loz[k] = z[k]; n.hiz[k] = z[4 + k];
+    }
     n.child[0] = g.x; n.child[1] = g.y; n.child[2] = g.z; n.child[3] = g.w;
 #else
     n = s.nodes4[node];
