@@ -179,6 +179,13 @@ def reference_sample(scene, cam, per_half: int, ref, seed: int, n_each: int = 1 
     return np.concatenate([camera, bounce])
 
 
+def headline_config(scene, world: int, log2_rays: int = LOG2_RAYS) -> dict:
+    """The workload description both arms print (the reference arm times a sample of it)."""
+    return {"workload": WORKLOAD, "rays_per_step": 1 << log2_rays, "triangles": int(len(scene.triangles)),
+            "bvh_nodes": int(len(scene.nodes)), "image": f"{WIDTH}x{HEIGHT}", "l2": "inputs larger than L2 (940 MB rays)",
+            "parallelism": f"replicas x{world}"}
+
+
 def cpu_reference_rate(scene, rays, ref, threads: int, chunk: int = 1 << 20):
     """Reference trace_world over `rays` on `threads` host threads, in chunks (bounded memory):
     (rays/s, seconds, per-ray mean box tests, per-ray mean primitive tests)."""
@@ -218,7 +225,7 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "sample": desc},
+        "config": headline_config(scene, args.gpus), "sample": desc,
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
                          "sample": desc + "; trace_world on host_view"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -1073,9 +1080,7 @@ def main(argv=None):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "rays_per_step": n, "triangles": int(len(scene.triangles)),
-                   "bvh_nodes": int(len(scene.nodes)), "image": f"{WIDTH}x{HEIGHT}", "l2": "inputs larger than L2 (940 MB rays)",
-                   "parallelism": f"replicas x{world}"},
+        "config": headline_config(scene, world, args.log2_rays),
         "kernel_ms": walk_ms, "kernel_stats_per_ray": {"child_boxes": stats[0], "primitives": stats[1]},
         "hit_rate": hit_rate, "scene_build_s": t_scene, "bvh": args.bvh, "gpu_bvh_build_s": t_gpu_build,
         "clocks": clock,
