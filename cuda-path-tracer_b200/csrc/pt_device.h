@@ -64,8 +64,12 @@ int device_sm_count();
 // takes at most this many persistent-kernel launches in flight at once.
 constexpr int kRayCounters = 64;
 
-// Tunables of the traversal kernels (pt_query_tuning; the autotuner sets them).
-struct QueryConfig { int persistent = 1; int min_active = 8; int blocks_per_sm = 0; int wide = 1; int speculative = 1; int order = 1; };
+// Tunables of the traversal kernels (pt_query_tuning and friends; process-wide).  Each field is
+// atomic, so a setter racing with launches on other threads is well defined; a launch reads each
+// field once.
+struct QueryConfig {
+    std::atomic<int> persistent{1}, min_active{8}, blocks_per_sm{0}, wide{1}, speculative{1}, order{1};
+};
 extern QueryConfig g_query_config;
 
 } // namespace ptb

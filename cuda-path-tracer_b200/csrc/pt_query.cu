@@ -260,7 +260,8 @@ void launch_query(const pt_scene *sc, const pt_ray *rays, size_t count, int mode
         Fn fn = table[k];
         const size_t smem = wide ? size_t(kSharedStack4) * kQueryBlock * sizeof(int2) : size_t(kSharedStack) * kQueryBlock * sizeof(int32_t);
         const int occupancy = blocks_per_sm(sc->device, k, (const void *)fn, smem);
-        int bps = g_query_config.blocks_per_sm > 0 ? std::min(g_query_config.blocks_per_sm, occupancy) : occupancy;
+        const int want_bps = g_query_config.blocks_per_sm;
+        int bps = want_bps > 0 ? std::min(want_bps, occupancy) : occupancy;
         size_t want = (count + kQueryBlock - 1) / kQueryBlock;
         unsigned grid = unsigned(std::min<size_t>(want, size_t(device_sm_count()) * size_t(bps > 0 ? bps : 1)));
         void *scratch = nullptr;
