@@ -480,6 +480,7 @@ def c3_record(args, hbm, l2_gbs, kind, check_rays: int = 1 << 16):
     par = closest_parity(scene, _gather(rays, idx, 28, pt.RAY), _gather(hits, idx, 16, pt.HIT), oracle, ref,
                          label=f"{len(idx)} seeded random rays of the 2^25")
     b_ray = 32 + 8 + 32 * par["n_box_reference"] + 48 * par["n_tri_reference"]
+    b_own = 32 + 8 + 32 * stats[0] + 48 * stats[1]
     walk_ms = float(np.mean(walk))
     out["closest"] = {"value": n * steps / (total / 1e3) / 1e9, "unit": UNIT, "steps": steps, "ms_per_step": total / steps,
                       "kernel_ms": walk_ms, "per_ray": {"child_boxes": stats[0], "primitives": stats[1]},
@@ -487,7 +488,13 @@ def c3_record(args, hbm, l2_gbs, kind, check_rays: int = 1 << 16):
                       "gpu_launches": steps * walk_launches_per_query(n), "parity": par,
                       "roofline": roofline_record(b_ray, n, walk_ms, hbm, l2_gbs, None, kind,
                                                   {"n_box": par["n_box_reference"], "n_tri": par["n_tri_reference"],
-                                                   "count_source": "the reference's trace_world on the parity sample"})}
+                                                   "count_source": "the reference's trace_world on the parity sample",
+                                                   "own_counts": {"bytes_per_ray": b_own,
+                                                                  "frac": b_own * n / (walk_ms / 1e3) / 1e9 / hbm,
+                                                                  "note": "the same formula on this kernel's own box and "
+                                                                          "primitive counts; the reference's depth-first walk "
+                                                                          "tests about twice as many boxes, which is why the "
+                                                                          "fraction above can exceed 1"}})}
     # any hit: shadow rays between surface points
     tmax = torch.empty(n * 4, dtype=torch.uint8, device="cuda")
     dev.surface_rays_device(5, 0, n, rays, tmax=tmax)
@@ -1064,8 +1071,11 @@ def main(argv=None):
     if parity:
         n_box, n_tri = parity["n_box_reference"], parity["n_tri_reference"]
         b_ray = 32 + 8 + 32 * n_box + 48 * n_tri
+        b_own = 32 + 8 + 32 * stats[0] + 48 * stats[1]
         roofline = roofline_record(b_ray, n, walk_ms, hbm, l2_gbs, traffic, peak_kind,
                                    {"n_box": n_box, "n_tri": n_tri,
+                                    "own_counts": {"bytes_per_ray": b_own, "frac": b_own * n / (walk_ms / 1e3) / 1e9 / hbm,
+                                                   "n_box": stats[0], "n_tri": stats[1]},
                                     "count_source": "the reference's trace_world on the parity sample (binary tree, "
                                                     "its own visiting order)",
                                     "hbm_read_probe_gbs": pt.read_bandwidth(4 << 30, 4) if rank == 0 else None,
