@@ -615,12 +615,14 @@ void merge_scenes(pt_batch *b, const pt_scene_desc *descs, int32_t count, std::v
         for (pt_light l : own) { l.primitive += l.type == PT_TRIANGLE ? tri_base : sphere_base; lights.push_back(l); }
     }
     b->total_triangles = triangles.size();
-    b->nodes4.upload(nodes4); b->nodes2.upload(nodes2); b->tris.upload(tris); b->spheres.upload(spheres); b->triangles.upload(triangles);
+    std::vector<Bvh4QNode> nodes4q;
+    for (const Bvh4Node &w : nodes4) nodes4q.push_back(quantize4(w));
+    b->nodes4.upload(nodes4q); b->nodes2.upload(nodes2); b->tris.upload(tris); b->spheres.upload(spheres); b->triangles.upload(triangles);
     b->sphere_src.upload(sphere_src); b->materials.upload(materials); b->textures.upload(textures);
     b->pixels.upload(pixels.data(), pixels.size()); b->lights.upload(lights);
     DeviceScene &v = b->view;
     v.nodes = nodes2.empty() ? nullptr : b->nodes2.get<BvhNode>();
-    v.nodes4 = nodes4.empty() ? nullptr : b->nodes4.get<Bvh4Node>();
+    v.nodes4 = nodes4.empty() ? nullptr : b->nodes4.get<Bvh4QNode>();
     v.tris = b->tris.get<TriRecord>(); v.spheres = b->spheres.get<SphereRecord>();
     v.triangles = b->triangles.get<pt_triangle>(); v.sphere_src = b->sphere_src.get<pt_sphere>();
     v.materials = b->materials.get<pt_material>(); v.textures = b->textures.get<pt_texture>();

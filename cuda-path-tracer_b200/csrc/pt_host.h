@@ -31,8 +31,10 @@ struct HostLayout {
     float root_lo[3] = {0, 0, 0}, root_hi[3] = {0, 0, 0};
     int32_t root_leaf = 0;
     std::vector<Bvh4Node> nodes4;       // empty when the flat graph shares subtrees
+    std::vector<Bvh4QNode> nodes4q;     // nodes4 quantized (what the device walks)
 };
 HostLayout relayout(const pt_scene_desc &scene);
+Bvh4QNode quantize4(const Bvh4Node &n);
 
 // Host-owned flattened scene (what the reference keeps in flat_scene).
 struct FlatScene {

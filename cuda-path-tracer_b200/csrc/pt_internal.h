@@ -41,16 +41,28 @@ static_assert(sizeof(BvhNode) == 64, "node is 64 bytes");
 // Four-wide node collapsed from the binary tree: the boxes of up to four children in SoA
 // (x/y/z min and max, four lanes each) and their references.  A child reference >= 0 is another
 // four-wide node; < 0 is a leaf of 1..8 consecutive slots, ~(first_slot << 3 | (count - 1));
-// kEmptyChild marks an unused lane (its box is inverted, so it never passes).  Padded to one
-// 128-byte cache line and aligned to it, so a node fetch touches one line and takes three 32-byte
-// loads and one 16-byte load.
-struct alignas(128) Bvh4Node {
+// kEmptyChild marks an unused lane (its box is inverted, so it never passes).  This is the form
+// the host builds; the device walks it quantized (Bvh4QNode).
+struct alignas(16) Bvh4Node {
     float lox[4], hix[4], loy[4], hiy[4], loz[4], hiz[4];
     int32_t child[4];
-    int32_t pad[4];
 };
-static_assert(sizeof(Bvh4Node) == 128, "four-wide node is one 128-byte line");
+static_assert(sizeof(Bvh4Node) == 112, "four-wide node is 112 bytes");
 constexpr int kLeafMax = 4;   // slots per four-wide leaf
+
+// Quantized four-wide node (64 bytes, half a cache line, two 32-byte loads): the children's boxes
+// on a per-axis power-of-two grid anchored at the low corner (px, py, pz) of their union, 8 bits
+// per bound, lower bounds rounded down and upper bounds up, so a dequantised box (p + q * 2^e)
+// always contains the child's true box.  The grid spacing is the smallest power of two with 255
+// steps covering the union.  An empty slot has its lower bounds above its upper ones.
+struct alignas(64) Bvh4QNode {
+    float px, py, pz;
+    uint32_t exps;                 // biased exponents of the grid spacing: x | y << 8 | z << 16
+    uint32_t qlo[3], qhi[3];       // per axis; child k in byte k
+    int32_t child[4];
+    uint32_t pad[2];
+};
+static_assert(sizeof(Bvh4QNode) == 64, "quantized four-wide node is 64 bytes");
 
 struct alignas(16) TriRecord {
     float v0x, v0y, v0z, eps;
@@ -68,7 +80,7 @@ static_assert(sizeof(SphereRecord) == 32, "sphere record is 32 bytes");
 // Everything a kernel needs, passed by value (device pointers).
 struct DeviceScene {
     const BvhNode *nodes;
-    const Bvh4Node *nodes4;         // null when the tree could not be collapsed (shared subtrees)
+    const Bvh4QNode *nodes4;        // null when the tree could not be collapsed (shared subtrees)
     const TriRecord *tris;
     const SphereRecord *spheres;
     const pt_triangle *triangles;   // caller's records (shading, light sampling)

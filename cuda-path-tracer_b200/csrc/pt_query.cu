@@ -359,7 +359,7 @@ pt_status pt_scene_create(const pt_scene_desc *desc, pt_scene **out) {
             sc->triangle_count = desc->triangle_count;
             sc->sphere_count = desc->sphere_count;
             sc->nodes.upload(layout.nodes);
-            sc->nodes4.upload(layout.nodes4);
+            sc->nodes4.upload(layout.nodes4q);
             sc->tris.upload(layout.tris);
             sc->spheres.upload(layout.spheres);
             sc->brute_order.upload(layout.brute_order);
@@ -372,7 +372,7 @@ pt_status pt_scene_create(const pt_scene_desc *desc, pt_scene **out) {
             sc->leaf_count = int32_t(layout.brute_order.size());
             DeviceScene &v = sc->view;
             v.nodes = sc->nodes.get<BvhNode>();
-            v.nodes4 = layout.nodes4.empty() ? nullptr : sc->nodes4.get<Bvh4Node>();
+            v.nodes4 = layout.nodes4q.empty() ? nullptr : sc->nodes4.get<Bvh4QNode>();
             v.tris = sc->tris.get<TriRecord>();
             v.spheres = sc->spheres.get<SphereRecord>();
             v.triangles = sc->triangles.get<pt_triangle>();

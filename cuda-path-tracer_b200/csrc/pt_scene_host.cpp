@@ -260,6 +260,38 @@ void build_wide(const pt_scene_desc &s, const std::vector<int32_t> &slot, int32_
 }
 } // namespace
 
+Bvh4QNode quantize4(const Bvh4Node &n) {
+    Bvh4QNode q{};
+    double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    const float *L[3] = {n.lox, n.loy, n.loz}, *H[3] = {n.hix, n.hiy, n.hiz};
+    for(int k = 0; k < 4; k++) {
+        q.child[k] = n.child[k];
+        if(n.child[k] == kEmptyChild) continue;
+        for(int a = 0; a < 3; a++) { lo[a] = std::min(lo[a], double(L[a][k])); hi[a] = std::max(hi[a], double(H[a][k])); }
+    }
+    float *P[3] = {&q.px, &q.py, &q.pz};
+    for(int a = 0; a < 3; a++) {
+        if(!(lo[a] <= hi[a])) { lo[a] = hi[a] = 0; }
+        *P[a] = float(lo[a]);
+        const double p = double(*P[a]), ext = hi[a] - p;
+        int e = ext > 0 ? int(std::ceil(std::log2(ext / 255.0))) : -126;
+        while(std::ldexp(255.0, e) < ext) e++;
+        e = std::max(-126, std::min(127, e));
+        const double step = std::ldexp(1.0, e);
+        q.exps |= uint32_t(e + 127) << (8 * a);
+        for(int k = 0; k < 4; k++) {
+            uint32_t ql = 255, qh = 0;   // an empty slot: inverted
+            if(n.child[k] != kEmptyChild) {
+                ql = uint32_t(std::min(255.0, std::max(0.0, std::floor((double(L[a][k]) - p) / step))));
+                qh = uint32_t(std::min(255.0, std::max(0.0, std::ceil((double(H[a][k]) - p) / step))));
+            }
+            q.qlo[a] |= ql << (8 * k);
+            q.qhi[a] |= qh << (8 * k);
+        }
+    }
+    return q;
+}
+
 // Re-layout: one 64-byte node per flat branch (reachable from the root), holding both
 // children's boxes; leaves become slots into the 48-byte triangle / 32-byte sphere arrays,
 // numbered in first-visit depth-first order so a subtree's leaves are contiguous.
@@ -365,6 +397,7 @@ HostLayout relayout(const pt_scene_desc &s) {
         }
         if(!shared) build_wide(s, slot, tri_slots, out);
     }
+    for(const Bvh4Node &w : out.nodes4) out.nodes4q.push_back(quantize4(w));
     // brute order: leaves in flat node-array order
     for(size_t id = 0; id < s.node_count; id++) {
         if(nodes[id].type == PT_BRANCH || slot[id] < 0) continue;

@@ -14,6 +14,7 @@
 // entry point, the last depth-first leaf (the reference's rule, transport.h:76-79).
 #pragma once
 
+#include <cstring>
 #include "pt_exact.h"
 
 namespace ptb {
@@ -518,11 +519,12 @@ namespace ptb {
 // new limit).
 // The box tests only filter: a primitive the walk never reaches could change the answer only if
 // the ray hit it at a point outside a box around it, and every box holds its primitives' boxes,
-// which the reference pads by 1e-4 on every axis (src/geometry/triangle.h:96-109).  So the slab
-// values are computed in one fused multiply-add each, t = box * (1/d) + (-o * (1/d)), whose
+// which the reference pads by 1e-4 on every axis (src/geometry/triangle.h:96-109).  So the walk
+// reads the children's boxes quantised outward to 8 bits per bound (Bvh4QNode, 64 bytes), and
+// computes each slab value in two fused multiply-adds, t = q * (2^e / d) + (p - o) / d, whose
 // rounding (a few ulps of t and of o/d) stays far inside that margin for scenes of up to a few
-// hundred units, and a box passes when entry <= exit.  A zero direction component is replaced
-// by +-1e-30 in the box test's inverse, so its slab accepts exactly the origins inside it.
+// hundred units; a box passes when entry <= exit.  A zero direction component is replaced by
+// +-1e-30 in the box test's inverse, so its slab accepts exactly the origins inside it.
 
 // Per-ray constants of the four-wide box test.
 struct RayBox4 {
@@ -573,37 +575,53 @@ __device__ __forceinline__ void ldg8(const float *p, float (&v)[8]) {
 }
 #endif
 
-PT_HD inline void load_node4(const DeviceScene &s, int32_t node, Bvh4Node &n) {
+PT_HD inline void load_node4(const DeviceScene &s, int32_t node, Bvh4QNode &n) {
 #ifdef __CUDA_ARCH__
-    const float *p = reinterpret_cast<const float *>(&s.nodes4[node]);   // 128-byte aligned
-    float x[8], y[8], z[8];
+    const float *p = reinterpret_cast<const float *>(&s.nodes4[node]);   // 64-byte records, 256-byte aligned base
+    float x[8], y[8];
     ldg8(p, x);
     ldg8(p + 8, y);
-    ldg8(p + 16, z);
-    const int4 g = __ldg(reinterpret_cast<const int4 *>(p + 24));
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-        n.lox[k] = x[k]; n.hix[k] = x[4 + k];
-        n.loy[k] = y[k]; n.hiy[k] = y[4 + k];
-        n.loz[k] = z[k]; n.hiz[k] = z[4 + k];
-    }
-    n.child[0] = g.x; n.child[1] = g.y; n.child[2] = g.z; n.child[3] = g.w;
+    n.px = x[0]; n.py = x[1]; n.pz = x[2]; n.exps = __float_as_uint(x[3]);
+    n.qlo[0] = __float_as_uint(x[4]); n.qlo[1] = __float_as_uint(x[5]); n.qlo[2] = __float_as_uint(x[6]);
+    n.qhi[0] = __float_as_uint(x[7]); n.qhi[1] = __float_as_uint(y[0]); n.qhi[2] = __float_as_uint(y[1]);
+    n.child[0] = __float_as_int(y[2]); n.child[1] = __float_as_int(y[3]); n.child[2] = __float_as_int(y[4]); n.child[3] = __float_as_int(y[5]);
 #else
     n = s.nodes4[node];
+#endif
+}
+
+// byte k of w as a float, exactly: the byte placed in the mantissa of 2^23, then 2^23 subtracted
+PT_HD inline float qbyte(uint32_t w, int k) {
+#ifdef __CUDA_ARCH__
+    return __int_as_float(int(__byte_perm(w, 0x4b000000u, 0x7540u + unsigned(k)))) - 8388608.0f;
+#else
+    return float((w >> (8 * k)) & 0xffu);
+#endif
+}
+PT_HD inline float exp2_of(uint32_t biased) {
+#ifdef __CUDA_ARCH__
+    return __int_as_float(int(biased << 23));
+#else
+    uint32_t bits = biased << 23; float f; std::memcpy(&f, &bits, 4); return f;
 #endif
 }
 
 // Tests the children of `node`; returns how many passed, in `ref`/`dist` sorted nearest first.
 PT_HD inline int node4_children(const DeviceScene &s, int32_t node, const RayBox4 &rb, float tmin, float limit,
                                 int32_t ref[4], float dist[4], uint32_t &boxes) {
-    Bvh4Node n;
+    Bvh4QNode n;
     load_node4(s, node, n);
+    const float sx = exp2_of(n.exps & 0xffu) * rb.jx, sy = exp2_of((n.exps >> 8) & 0xffu) * rb.jy, sz = exp2_of((n.exps >> 16) & 0xffu) * rb.jz;
+    const float tx = fma_box(n.px, rb.jx, rb.kx), ty = fma_box(n.py, rb.jy, rb.ky), tz = fma_box(n.pz, rb.jz, rb.kz);
+    const uint32_t nxw = rb.nx ? n.qhi[0] : n.qlo[0], fxw = rb.nx ? n.qlo[0] : n.qhi[0];
+    const uint32_t nyw = rb.ny ? n.qhi[1] : n.qlo[1], fyw = rb.ny ? n.qlo[1] : n.qhi[1];
+    const uint32_t nzw = rb.nz ? n.qhi[2] : n.qlo[2], fzw = rb.nz ? n.qlo[2] : n.qhi[2];
     int hits = 0;
 #pragma unroll
     for (int k = 0; k < 4; k++) {
-        const float ax = fma_box(rb.nx ? n.hix[k] : n.lox[k], rb.jx, rb.kx), bx = fma_box(rb.nx ? n.lox[k] : n.hix[k], rb.jx, rb.kx);
-        const float ay = fma_box(rb.ny ? n.hiy[k] : n.loy[k], rb.jy, rb.ky), by = fma_box(rb.ny ? n.loy[k] : n.hiy[k], rb.jy, rb.ky);
-        const float az = fma_box(rb.nz ? n.hiz[k] : n.loz[k], rb.jz, rb.kz), bz = fma_box(rb.nz ? n.loz[k] : n.hiz[k], rb.jz, rb.kz);
+        const float ax = fma_box(qbyte(nxw, k), sx, tx), bx = fma_box(qbyte(fxw, k), sx, tx);
+        const float ay = fma_box(qbyte(nyw, k), sy, ty), by = fma_box(qbyte(fyw, k), sy, ty);
+        const float az = fma_box(qbyte(nzw, k), sz, tz), bz = fma_box(qbyte(fzw, k), sz, tz);
         const float entry = fmaxf(max3(ax, ay, az), tmin), exit = fminf(min3(bx, by, bz), limit);
         const bool h = n.child[k] != kEmptyChild && entry <= exit;
         boxes += n.child[k] != kEmptyChild;

@@ -228,7 +228,7 @@ pt_status pt_add_samples(pt_renderer *renderer, int count);
 pt_status pt_set_block_shape(pt_renderer *renderer, int width, int height);
 /* Live-path count below which add_samples stops the wavefront and runs the remaining paths to
  * completion in one fused kernel (two threads per path on four-wide trees: one walks the path's
- * next ray while the other walks its last shadow ray; default max(16384, pixels/4); 0 keeps the
+ * next ray while the other walks its last shadow ray; default max(65536, pixels/4); 0 keeps the
  * wavefront to the end).  Results do not depend on it. */
 pt_status pt_renderer_tuning(pt_renderer *renderer, int32_t tail_paths);
 /* Linear FP32 radiance sums (3 floats per pixel, row 0 at the bottom, not divided by spp). */
