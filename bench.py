@@ -97,9 +97,10 @@ def measured_peaks():
     return 6650.0, 1590.0, "fallback"
 
 
-def profile_summary():
-    """Figures of the committed ncu summary of the walk kernel (profiles/query_walk_ncu.json)."""
-    p = ROOT / "profiles" / "query_walk_ncu.json"
+def profile_summary(name: str = "query_walk_ncu.json"):
+    """Figures of a committed ncu summary of the walk kernel (profiles/query_walk_ncu.json for
+    config 2, profiles/query_microbenchmark_ncu.json for config 3)."""
+    p = ROOT / "profiles" / name
     return json.loads(p.read_text()) if p.exists() else {}
 
 
@@ -486,7 +487,9 @@ def c3_record(args, hbm, l2_gbs, kind, check_rays: int = 1 << 16):
                       "kernel_ms": walk_ms, "per_ray": {"child_boxes": stats[0], "primitives": stats[1]},
                       "hit_rate": float((hits.view(torch.int32).view(-1, 4)[:, 2] != 0).float().mean().item()),
                       "gpu_launches": steps * walk_launches_per_query(n), "parity": par,
-                      "roofline": roofline_record(b_ray, n, walk_ms, hbm, l2_gbs, None, kind,
+                      "roofline": roofline_record(b_ray, n, walk_ms, hbm, l2_gbs,
+                                                  profile_summary("query_microbenchmark_ncu.json").get("bytes_per_launch_2^25")
+                                                  if n == 1 << 25 else None, kind,
                                                   {"n_box": par["n_box_reference"], "n_tri": par["n_tri_reference"],
                                                    "count_source": "the reference's trace_world on the parity sample",
                                                    "own_counts": {"bytes_per_ray": b_own,
