@@ -598,7 +598,8 @@ def run_batch(args):
 
 def mlp_timings(net, n_query: int = 1 << 21, n_train: int = 1 << 16, reps: int = 20):
     """CUDA-event times of the radiance-cache network alone: a forward pass over n_query
-    queries and one Adam step (forward + backward + reduce + update) over n_train samples,
+    queries and one Adam step (forward + backward in one launch, then the reduction with the
+    update in a second) over n_train samples,
     on seeded synthetic queries in a 10-unit box."""
     import torch
     q = torch.zeros((n_query, 13), dtype=torch.float32, device="cuda")
@@ -630,7 +631,7 @@ def mlp_timings(net, n_query: int = 1 << 21, n_train: int = 1 << 16, reps: int =
     return {"forward_queries": n_query, "forward_ms": fwd_ms, "forward_tflops": fwd_tf, "train_samples": n_train,
             "train_step_ms": train_ms, "train_tflops": train_tf, "flop_per_query": 41344,
             "flop_per_training_sample": 3 * 41344, "peak_tflops": tpeak,
-            "peak_kind": kind, "launches_per_rep": {"forward": 1, "train": 3}}
+            "peak_kind": kind, "launches_per_rep": {"forward": 1, "train": 2}}
 
 
 def run_mlp(args):
@@ -647,7 +648,7 @@ def run_mlp(args):
             "config": {"workload": "MLP 64-64x5-3 forward over 2^21 queries; Adam step over 2^16 samples"},
             "roofline": {"bound": "tensor", "achieved": m["forward_tflops"], "peak": m["peak_tflops"], "unit": "TFLOP/s",
                          "frac": m["forward_tflops"] / m["peak_tflops"], "traffic": None, "peak_kind": m["peak_kind"]},
-            "mlp": m, "clocks": clock, "gpu_launches": 4 * (max(1, args.steps) + 3)}
+            "mlp": m, "clocks": clock, "gpu_launches": 3 * (max(1, args.steps) + 3)}
     print(json.dumps(line), flush=True)
 
 

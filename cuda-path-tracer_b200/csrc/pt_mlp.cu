@@ -514,26 +514,6 @@ __global__ void __launch_bounds__(kTile, 1) train_kernel(const unsigned char *we
     tmem_free(tbase, 512);
 }
 
-// Sums the per-CTA partials in a fixed order (deterministic) into `grad`; thread 0 also sums the
-// loss partials into loss[0] (mean) and, for a training step (advance) on a non-empty batch,
-// advances the Adam step (step[0]) and the weight-average step (step[1]).
-__global__ void reduce_kernel(const float *partial, const float *loss_partial, int ctas, size_t count, const int32_t *count_dev,
-                              float *grad, float *loss, int *step, int advance, const int *status) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (*status) return;                          // the gradients kernel timed out: no step
-    if (i == 0) {
-        size_t n = count_dev ? min(count, size_t(max(0, *count_dev))) : count;
-        float l = 0.0f;
-        for (int c = 0; c < ctas; c++) l += loss_partial[c];
-        loss[0] = n ? l / float(n * kOut) : 0.0f;
-        if (n && advance) { step[0] += 1; step[1] += 1; }
-    }
-    if (i >= kMasterFloats) return;
-    float s = 0.0f;
-    for (int c = 0; c < ctas; c++) s += partial[size_t(c) * kMasterFloats + i];
-    grad[i] = s;
-}
-
 // FP32 master weight i -> its bf16 position in the canonical buffer.
 __host__ __device__ inline uint32_t master_to_canon(int i) {
     if (i < kHidden * 4096) {
@@ -544,31 +524,77 @@ __host__ __device__ inline uint32_t master_to_canon(int i) {
     return uint32_t(kHidden * kMatBytes) + canon(uint32_t(n), uint32_t(k), 64);
 }
 
-// Adam (bias-corrected) on the FP32 masters; writes the bf16 canonical copy.
-// The step count lives on the device so that a captured graph replays with the right bias
-// correction; an empty batch (count_dev == 0) leaves the weights alone.  With ema_decay > 0 the
-// kernel also keeps the exponential moving average of the weights (bias-corrected, as Adam's
-// moments are) and writes its bf16 copy, the weights that inference uses.
-__global__ void adam_kernel(float *master, float *m, float *v, const float *grad, const int *step_dev, const int32_t *count_dev,
-                            float lr, float beta1, float beta2, float eps, unsigned char *canon_out, float ema_decay,
-                            float *ema, unsigned char *ema_canon, const int *status) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= kMasterFloats || (count_dev && *count_dev <= 0) || *status) return;
-    const int step = step_dev[0];
-    float g = grad[i];
-    float mi = beta1 * m[i] + (1.0f - beta1) * g;
-    float vi = beta2 * v[i] + (1.0f - beta2) * g * g;
-    m[i] = mi; v[i] = vi;
-    float mh = mi / (1.0f - powf(beta1, float(step))), vh = vi / (1.0f - powf(beta2, float(step)));
-    float w = master[i] - lr * mh / (sqrtf(vh) + eps);
-    master[i] = w;
-    const uint32_t at = master_to_canon(i);
-    *reinterpret_cast<__nv_bfloat16 *>(canon_out + at) = __float2bfloat16_rn(w);
-    if (ema_decay > 0.0f) {
-        float e = ema_decay * ema[i] + (1.0f - ema_decay) * w;
-        ema[i] = e;
-        float corrected = e / (1.0f - powf(ema_decay, float(step_dev[1])));
-        *reinterpret_cast<__nv_bfloat16 *>(ema_canon + at) = __float2bfloat16_rn(corrected);
+struct AdamArgs {
+    float *master, *m, *v;
+    float lr, beta1, beta2, eps;
+    unsigned char *canon_out;           // bf16 canonical copy of the masters
+    float ema_decay;                    // > 0: also keep the weight average and its bf16 copy
+    float *ema;
+    unsigned char *ema_canon;
+};
+
+constexpr int kReduceSlices = 8;        // warps per block; warp k sums the partials of CTAs k, k + 8, ...
+
+// Sums the per-CTA partial gradients into `grad` and, with kAdam on a non-empty batch, applies
+// one bias-corrected Adam step to the FP32 masters and writes their bf16 canonical copy (and the
+// weight average with its copy).  One block of 8 warps per 32 masters: warp k sums the rows of
+// CTAs k, k + 8, ... (each row read as one 128-byte line), then warp 0 adds the eight sums in a
+// fixed order, so the result is deterministic.  Every block reads the step counters as they were
+// before this step and uses step + 1; the last block to finish (completion counter `done`, reset
+// by that block) writes the mean loss into loss[0] and, with `advance` on a non-empty batch,
+// advances the Adam step (step[0]) and the weight-average step (step[1]).  Nothing happens when
+// the gradient kernel timed out (*status).
+template <bool kAdam>
+__global__ void __launch_bounds__(32 * kReduceSlices) reduce_step_kernel(const float *partial, const float *loss_partial, int ctas,
+                                                                         size_t count, const int32_t *count_dev, float *grad,
+                                                                         float *loss, int *step, unsigned *done, int advance,
+                                                                         AdamArgs a, const int *status) {
+    if (*status) return;
+    __shared__ float sums[kReduceSlices][32];
+    __shared__ bool last;
+    const int lane = threadIdx.x & 31, slice = threadIdx.x >> 5;
+    const int i = blockIdx.x * 32 + lane;
+    const size_t n = count_dev ? min(count, size_t(max(0, *count_dev))) : count;
+    float s = 0.0f;
+    if (i < kMasterFloats)
+        for (int c = slice; c < ctas; c += kReduceSlices) s += partial[size_t(c) * kMasterFloats + i];
+    sums[slice][lane] = s;
+    __syncthreads();
+    if (slice == 0 && i < kMasterFloats) {
+        float g = sums[0][lane];
+#pragma unroll
+        for (int k = 1; k < kReduceSlices; k++) g += sums[k][lane];
+        grad[i] = g;
+        if (kAdam && n) {
+            const int t = step[0] + 1;
+            float mi = a.beta1 * a.m[i] + (1.0f - a.beta1) * g;
+            float vi = a.beta2 * a.v[i] + (1.0f - a.beta2) * g * g;
+            a.m[i] = mi; a.v[i] = vi;
+            float mh = mi / (1.0f - powf(a.beta1, float(t))), vh = vi / (1.0f - powf(a.beta2, float(t)));
+            float w = a.master[i] - a.lr * mh / (sqrtf(vh) + a.eps);
+            a.master[i] = w;
+            const uint32_t at = master_to_canon(i);
+            *reinterpret_cast<__nv_bfloat16 *>(a.canon_out + at) = __float2bfloat16_rn(w);
+            if (a.ema_decay > 0.0f) {
+                float e = a.ema_decay * a.ema[i] + (1.0f - a.ema_decay) * w;
+                a.ema[i] = e;
+                float corrected = e / (1.0f - powf(a.ema_decay, float(step[1] + 1)));
+                *reinterpret_cast<__nv_bfloat16 *>(a.ema_canon + at) = __float2bfloat16_rn(corrected);
+            }
+        }
+    }
+    __syncthreads();                    // this block's reads of step[] are done
+    if (threadIdx.x == 0) {
+        __threadfence();
+        last = atomicAdd(done, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        float l = 0.0f;
+        for (int c = 0; c < ctas; c++) l += loss_partial[c];
+        loss[0] = n ? l / float(n * kOut) : 0.0f;
+        if (n && advance) { step[0] += 1; step[1] += 1; }
+        *done = 0;
     }
 }
 
@@ -585,6 +611,7 @@ using namespace ptb::mlp;
 
 struct pt_cache {
     DeviceBuffer master, adam_m, adam_v, grad, weights, partial, loss_partial, status, step, loss;
+    DeviceBuffer done;                  // completion counter of the reduction (zero between launches)
     DeviceBuffer ema, ema_weights;      // weight average and its bf16 copy (used for inference when ema_decay > 0)
     float lo[3], hi[3];
     int ctas = 0;
@@ -613,8 +640,9 @@ void check_status(pt_cache *c) {
 }
 float3 lo3(const pt_cache *c) { return make_float3(c->lo[0], c->lo[1], c->lo[2]); }
 float3 hi3(const pt_cache *c) { return make_float3(c->hi[0], c->hi[1], c->hi[2]); }
-// forward/backward/reduce into c->grad and c->loss; no host synchronisation
-void gradients(pt_cache *c, const pt_cache_query *q, const float *targets, size_t count, const int32_t *count_dev, bool advance,
+// forward/backward/reduce into c->grad and c->loss and, for a training step, the Adam update in
+// the same reduction launch; no host synchronisation
+void gradients(pt_cache *c, const pt_cache_query *q, const float *targets, size_t count, const int32_t *count_dev, bool train,
                cudaStream_t st) {
     size_t tiles = (count + kTile - 1) / kTile;
     int grid = count_dev ? c->ctas : int(std::min<size_t>(tiles ? tiles : 1, size_t(c->ctas)));
@@ -622,9 +650,13 @@ void gradients(pt_cache *c, const pt_cache_query *q, const float *targets, size_
                                                    c->partial.get<float>(), c->loss_partial.get<float>(), c->status.get<int>(),
                                                    c->attempts);
     PT_CUDA(cudaGetLastError());
-    reduce_kernel<<<(kMasterFloats + 255) / 256, 256, 0, st>>>(c->partial.get<float>(), c->loss_partial.get<float>(), grid, count,
-                                                               count_dev, c->grad.get<float>(), c->loss.get<float>(), c->step.get<int>(),
-                                                               advance ? 1 : 0, c->status.get<int>());
+    AdamArgs a{c->master.get<float>(), c->adam_m.get<float>(), c->adam_v.get<float>(), c->lr, c->beta1, c->beta2, c->eps,
+               c->weights.get<unsigned char>(), c->ema_decay, c->ema.get<float>(), c->ema_weights.get<unsigned char>()};
+    const unsigned blocks = unsigned((kMasterFloats + 31) / 32);
+    auto kernel = train ? reduce_step_kernel<true> : reduce_step_kernel<false>;
+    kernel<<<blocks, 32 * kReduceSlices, 0, st>>>(c->partial.get<float>(), c->loss_partial.get<float>(), grid, count, count_dev,
+                                                   c->grad.get<float>(), c->loss.get<float>(), c->step.get<int>(),
+                                                   c->done.get<unsigned>(), train ? 1 : 0, a, c->status.get<int>());
     PT_CUDA(cudaGetLastError());
 }
 float read_loss(pt_cache *c, cudaStream_t st) {
@@ -652,12 +684,6 @@ void cache_train(pt_cache *c, const pt_cache_query *queries, const float *target
                  cudaStream_t st) {
     if (!count) return;
     gradients(c, queries, targets, count, count_dev, true, st);
-    adam_kernel<<<(kMasterFloats + 255) / 256, 256, 0, st>>>(c->master.get<float>(), c->adam_m.get<float>(), c->adam_v.get<float>(),
-                                                             c->grad.get<float>(), c->step.get<int>(), count_dev, c->lr, c->beta1,
-                                                             c->beta2, c->eps, c->weights.get<unsigned char>(), c->ema_decay,
-                                                             c->ema.get<float>(), c->ema_weights.get<unsigned char>(),
-                                                             c->status.get<int>());
-    PT_CUDA(cudaGetLastError());
 }
 float cache_loss(pt_cache *c, cudaStream_t st) { return read_loss(c, st); }
 void cache_status(pt_cache *c) { check_status(c); }
@@ -702,6 +728,8 @@ pt_status pt_cache_create(const float scene_lo[3], const float scene_hi[3], uint
             PT_CUDA(cudaMemset(c->status.get(), 0, sizeof(int)));
             c->step.resize(2 * sizeof(int));
             PT_CUDA(cudaMemset(c->step.get(), 0, 2 * sizeof(int)));
+            c->done.resize(sizeof(unsigned));
+            PT_CUDA(cudaMemset(c->done.get(), 0, sizeof(unsigned)));
             c->loss.resize(sizeof(float));
             PT_CUDA(cudaMemset(c->loss.get(), 0, sizeof(float)));
             PT_CUDA(cudaFuncSetAttribute(forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kFwdSmem)));

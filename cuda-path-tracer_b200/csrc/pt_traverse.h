@@ -675,7 +675,9 @@ PT_HD inline bool traverse4_rt(const DeviceScene &s, const pt_ray &r, float tmin
             int hits = node4_children(s, cur, rb, tmin, limit, ref, dist, boxes);
             if (hits) {
                 if (sp + hits - 1 > 3 * kStackCapacity) { error = 1; hit.slot = -1; return false; }
-                for (int k = hits - 1; k >= 1; k--) { sref[sp] = ref[k]; sdist[sp] = dist[k]; sp++; }
+#pragma unroll
+                for (int k = 3; k >= 1; k--)           // static indices: ref/dist stay in registers
+                    if (k < hits) { sref[sp] = ref[k]; sdist[sp] = dist[k]; sp++; }
                 cur = ref[0];
                 continue;
             }
@@ -767,10 +769,13 @@ __device__ inline void persistent_walk4(const DeviceScene &s, size_t count, unsi
                     if (hits) {
                         if (sp + hits - 1 > kStack4) { error = 1; found = false; end = true; }
                         else {
-                            for (int k = hits - 1; k >= 1; k--) {
-                                int2 e = make_int2(ref[k], __float_as_int(dist[k]));
-                                if (sp < kSharedStack4) my_stack[sp * stride] = e; else spill[sp - kSharedStack4] = e;
-                                sp++;
+#pragma unroll
+                            for (int k = 3; k >= 1; k--) {    // static indices: ref/dist stay in registers
+                                if (k < hits) {
+                                    int2 e = make_int2(ref[k], __float_as_int(dist[k]));
+                                    if (sp < kSharedStack4) my_stack[sp * stride] = e; else spill[sp - kSharedStack4] = e;
+                                    sp++;
+                                }
                             }
                             cur = ref[0];
                             descended = true;
@@ -889,10 +894,13 @@ __device__ inline void persistent_walk4_spec(const DeviceScene &s, size_t count,
                     if (hits) {
                         if (sp + hits - 1 > kStack4) { error = 1; cur = kNone; leaf = kNone; }
                         else {
-                            for (int k = hits - 1; k >= 1; k--) {
-                                int2 e = make_int2(ref[k], __float_as_int(dist[k]));
-                                if (sp < kSharedStack4) my_stack[sp * stride] = e; else spill[sp - kSharedStack4] = e;
-                                sp++;
+#pragma unroll
+                            for (int k = 3; k >= 1; k--) {    // static indices: ref/dist stay in registers
+                                if (k < hits) {
+                                    int2 e = make_int2(ref[k], __float_as_int(dist[k]));
+                                    if (sp < kSharedStack4) my_stack[sp * stride] = e; else spill[sp - kSharedStack4] = e;
+                                    sp++;
+                                }
                             }
                             cur = ref[0];
                         }
