@@ -52,7 +52,6 @@ LOG2_RAYS = 25
 WORKLOAD = "procedural-1M-triangles closest-hit, 2^24 camera + 2^24 bounce rays"
 # CUB's stable radix sort of 30-bit keys: 4 onesweep passes + a histogram + an exclusive sum
 SORT_LAUNCHES = 6
-ORDER_MIN_RAYS = 1 << 18
 
 
 def parse(argv=None):
@@ -278,10 +277,11 @@ def whole_job_rate(world: int, units_per_rank: int, steps: int, max_seconds: flo
     return world * units_per_rank * steps / max_seconds
 
 
-def walk_launches_per_query(count: int) -> int:
+def walk_launches_per_query(ordered: bool) -> int:
     """Kernels one query_device call launches: the walk, plus the ray-key kernel and the sort's
-    kernels when the batch is walked in key order."""
-    return 1 + (1 + SORT_LAUNCHES if count >= ORDER_MIN_RAYS else 0)
+    kernels when the batch is walked in key order (Scene.query_ordered: batches of at least
+    2^18 rays on scenes whose walked arrays exceed the L2, under the default setting)."""
+    return 1 + (1 + SORT_LAUNCHES if ordered else 0)
 
 
 # --------------------------------------------------------------------------------------- parity
@@ -486,7 +486,7 @@ def c3_record(args, hbm, l2_gbs, kind, check_rays: int = 1 << 16):
     out["closest"] = {"value": n * steps / (total / 1e3) / 1e9, "unit": UNIT, "steps": steps, "ms_per_step": total / steps,
                       "kernel_ms": walk_ms, "per_ray": {"child_boxes": stats[0], "primitives": stats[1]},
                       "hit_rate": float((hits.view(torch.int32).view(-1, 4)[:, 2] != 0).float().mean().item()),
-                      "gpu_launches": steps * walk_launches_per_query(n), "parity": par,
+                      "gpu_launches": steps * walk_launches_per_query(dev.query_ordered(n)), "parity": par,
                       "roofline": roofline_record(b_ray, n, walk_ms, hbm, l2_gbs,
                                                   profile_summary("query_microbenchmark_ncu.json").get("bytes_per_launch_2^25")
                                                   if n == 1 << 25 else None, kind,
@@ -514,7 +514,7 @@ def c3_record(args, hbm, l2_gbs, kind, check_rays: int = 1 << 16):
                   "kernel_ms": walk_ms, "per_ray": {"child_boxes": stats[0], "primitives": stats[1]},
                   "occluded_rate": float((hits.view(torch.int32).view(-1, 4)[:, 2] != 0).float().mean().item()),
                   "rays": "2^25 shadow rays between two random surface points, tmax = distance - 0.001",
-                  "gpu_launches": steps * walk_launches_per_query(n), "parity": par,
+                  "gpu_launches": steps * walk_launches_per_query(dev.query_ordered(n)), "parity": par,
                   "roofline": roofline_record(b_ray, n, walk_ms, hbm, l2_gbs, None, kind,
                                               {"n_box": stats[0], "n_tri": stats[1],
                                                "count_source": "this kernel's own counters (the reference has no "
@@ -1089,7 +1089,7 @@ def main(argv=None):
     if extras and not args.no_ref_gpu:
         ref_gpu = guarded("reference_gpu", reference_gpu_record, scene, dev, rays, n, value)
 
-    launches = walk_launches_per_query(n)
+    launches = walk_launches_per_query(dev.query_ordered(n))
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,

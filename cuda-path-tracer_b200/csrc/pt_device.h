@@ -68,7 +68,8 @@ constexpr int kRayCounters = 64;
 // atomic, so a setter racing with launches on other threads is well defined; a launch reads each
 // field once.
 struct QueryConfig {
-    std::atomic<int> persistent{1}, min_active{8}, blocks_per_sm{0}, wide{1}, speculative{1}, order{1};
+    std::atomic<int> persistent{1}, min_active{24}, blocks_per_sm{0}, wide{1}, speculative{1};
+    std::atomic<int> order{2};             // 0 never, 1 always, 2 when the walked arrays exceed the L2
 };
 extern QueryConfig g_query_config;
 
@@ -90,6 +91,7 @@ struct pt_scene {
     std::atomic<unsigned> counter_slot{0};
     cudaMemPool_t order_pool = nullptr;     // stream-ordered scratch of the ray ordering (kept, not released)
     int device = 0;
+    size_t l2_bytes = 0;                    // L2 size of the scene's device (the ray ordering's threshold)
     // pt_query_profile: CUDA events recorded around each walk-kernel launch (pairs, a ring)
     std::vector<cudaEvent_t> profile_events;
     size_t profile_next = 0;

@@ -197,6 +197,15 @@ __global__ void ray_keys_kernel(const pt_ray *__restrict__ rays, size_t count, f
 // Sorts the batch's ray indices by key into scratch from the scene's memory pool (allocated and
 // freed in stream order, so concurrent queries on other streams get their own).  Returns the
 // order and the scratch to free after the walk.
+// Ordering pays when the walked arrays do not fit in L2 (the walk is then bound by its node and
+// triangle fetches); with an L2-resident tree the sort costs more than it saves.
+bool walks_ordered(const pt_scene *sc, bool wide, size_t count) {
+    const size_t walk_bytes = (wide ? sc->nodes4.bytes() : sc->nodes.bytes()) + sc->tris.bytes() + sc->spheres.bytes();
+    const int mode = g_query_config.order;
+    const bool ordered = mode == 1 || (mode == 2 && walk_bytes > sc->l2_bytes);
+    return ordered && count >= kOrderMin && count <= size_t(INT32_MAX) && sc->order_pool;
+}
+
 const uint32_t *order_rays(const pt_scene *sc, const pt_ray *rays, size_t count, cudaStream_t stream, void *&scratch) {
     const DeviceScene &s = sc->view;
     float3 lo = make_float3(s.root_lo[0], s.root_lo[1], s.root_lo[2]);
@@ -266,7 +275,7 @@ void launch_query(const pt_scene *sc, const pt_ray *rays, size_t count, int mode
         unsigned grid = unsigned(std::min<size_t>(want, size_t(device_sm_count()) * size_t(bps > 0 ? bps : 1)));
         void *scratch = nullptr;
         const uint32_t *order = nullptr;
-        if (g_query_config.order && count >= kOrderMin && count <= size_t(INT32_MAX) && sc->order_pool) {
+        if (walks_ordered(sc, wide, count)) {
             cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
             PT_CUDA(cudaStreamIsCapturing(stream, &capture));
             if (capture == cudaStreamCaptureStatusNone) order = order_rays(sc, rays, count, stream, scratch);   // not inside a graph capture
@@ -344,6 +353,11 @@ pt_status pt_scene_create(const pt_scene_desc *desc, pt_scene **out) {
         auto sc = new pt_scene;
         try {
             PT_CUDA(cudaGetDevice(&sc->device));
+            {
+                int l2 = 0;
+                PT_CUDA(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, sc->device));
+                sc->l2_bytes = size_t(l2 > 0 ? l2 : 0);
+            }
             {   // the ray ordering's scratch pool: memory stays with the pool between queries
                 cudaMemPoolProps props{};
                 props.allocType = cudaMemAllocationTypePinned;
@@ -402,6 +416,14 @@ pt_status pt_scene_lights(const pt_scene *scene, pt_light *lights, size_t capaci
         if(count) *count = scene->host_lights.size();
         if(total_area) *total_area = scene->light_area;
         for(size_t i = 0; i < capacity && i < scene->host_lights.size(); i++) lights[i] = scene->host_lights[i];
+    });
+}
+
+pt_status pt_query_ordered(const pt_scene *s, size_t count, int *ordered) {
+    return guard([&]() {
+        if(!s || !ordered) throw Error(PT_INVALID_ARGUMENT, "null argument");
+        const bool wide = g_query_config.wide && s->view.nodes4;
+        *ordered = g_query_config.persistent && walks_ordered(s, wide, count) ? 1 : 0;
     });
 }
 
@@ -514,9 +536,13 @@ pt_status pt_query_walk(int speculative) {
     return guard([&]() { g_query_config.speculative = speculative ? 1 : 0; });
 }
 
-// Ray ordering of large batches: 1 = walk rays in (octant, origin Morton code) order, 0 = as given.
-pt_status pt_query_order(int enabled) {
-    return guard([&]() { g_query_config.order = enabled ? 1 : 0; });
+// Ray ordering of large batches: 1 = walk rays in (octant, origin Morton code) order, 0 = as given,
+// 2 = ordered only when the scene's walked arrays exceed the device's L2.
+pt_status pt_query_order(int mode) {
+    return guard([&]() {
+        if (mode < 0 || mode > 2) throw Error(PT_INVALID_ARGUMENT, "ray ordering mode must be 0, 1 or 2");
+        g_query_config.order = mode;
+    });
 }
 
 // Walk-kernel timing: `launches` > 0 creates that many event pairs (recorded around each later

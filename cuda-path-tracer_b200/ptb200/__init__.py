@@ -111,6 +111,7 @@ def library() -> C.CDLL:
         "pt_scene_destroy": (I, [P]),
         "pt_scene_lights": (I, [P, P, S, P, P]),
         "pt_scene_device_bytes": (I, [P, P]),
+        "pt_query_ordered": (I, [P, S, P]),
         "pt_query_rays_device": (I, [P, P, S, I, F, P, P, P, P]),
         "pt_query_rays_brute_device": (I, [P, P, S, I, F, P, P, P, P]),
         "pt_query_rays": (I, [P, P, S, I, F, P, P, P]),
@@ -447,6 +448,12 @@ class Scene:
         check(library().pt_scene_device_bytes(self._h, C.byref(n)))
         return n.value
 
+    def query_ordered(self, count: int) -> bool:
+        """Whether a query of `count` rays is walked in key order under the current settings (pt_query_ordered)."""
+        o = C.c_int()
+        check(library().pt_query_ordered(self._h, int(count), C.byref(o)))
+        return bool(o.value)
+
     def query(self, rays: np.ndarray, mode: int = QUERY_CLOSEST, tmin: float = 0.001, tmax=None, stats=False):
         """Host-buffer query (pt_query_rays): returns HIT records (and RAY_STATS)."""
         rays = np.ascontiguousarray(rays, RAY)
@@ -500,7 +507,7 @@ def read_bandwidth(nbytes: int, reps: int = 20) -> float:
     return g.value
 
 
-def query_tuning(persistent: int = 1, min_active: int = 8, blocks_per_sm: int = 0) -> None:
+def query_tuning(persistent: int = 1, min_active: int = 24, blocks_per_sm: int = 0) -> None:
     """Sets the ray-query kernel variant and its tunables (pt_query_tuning)."""
     check(library().pt_query_tuning(persistent, min_active, blocks_per_sm))
 
@@ -515,9 +522,10 @@ def query_walk(speculative: int = 1) -> None:
     check(library().pt_query_walk(int(speculative)))
 
 
-def query_order(enabled: int = 1) -> None:
-    """Ray ordering of large batches by (octant, origin Morton code) (pt_query_order)."""
-    check(library().pt_query_order(int(enabled)))
+def query_order(mode: int = 2) -> None:
+    """Ray ordering of large batches by (octant, origin Morton code) (pt_query_order): 0 never,
+    1 always, 2 when the scene's walked arrays exceed the L2 (default)."""
+    check(library().pt_query_order(int(mode)))
 
 
 def cuda_query_rays(scene: FlatScene, rays: np.ndarray, brute: bool = False) -> np.ndarray:

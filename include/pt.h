@@ -123,6 +123,9 @@ pt_status pt_scene_destroy(pt_scene *scene);
 pt_status pt_scene_lights(const pt_scene *scene, pt_light *lights, size_t capacity, size_t *count, float *total_area);
 /* Device bytes held by the scene (nodes, triangles, shading records, lights). */
 pt_status pt_scene_device_bytes(const pt_scene *scene, size_t *bytes);
+/* Whether a query of `count` rays on this scene is walked in key order under the current
+ * pt_query_order setting (*ordered = 1: a key kernel and a radix sort run before the walk). */
+pt_status pt_query_ordered(const pt_scene *scene, size_t count, int *ordered);
 
 /* ---- ray queries ----
  * Closest hit follows trace_world(…, brute=false) (src/renderer/transport.h:43-85) with
@@ -173,7 +176,7 @@ pt_status pt_query_rays_brute_device(const pt_scene *scene, const pt_ray *rays, 
 /* Tuning of the ray-query kernel (process-wide): persistent = 1 runs a fixed grid of warps that
  * take rays from a global counter and refill lanes whose ray has ended once fewer than
  * `min_active` (1..32) lanes are busy; persistent = 0 launches one thread per ray.
- * blocks_per_sm = 0 uses the occupancy limit.  Defaults: 1, 8, 0. */
+ * blocks_per_sm = 0 uses the occupancy limit.  Defaults: 1, 24, 0. */
 pt_status pt_query_tuning(int persistent, int min_active, int blocks_per_sm);
 /* Node layout of the traversal kernels (process-wide; renderers pick it up when created):
  * 1 = four-wide nodes (up to 4 primitives per leaf) where the scene's tree allows it (default),
@@ -184,9 +187,12 @@ pt_status pt_query_layout(int wide);
 pt_status pt_query_walk(int speculative);
 /* Ray ordering (process-wide): 1 = batches of at least 2^18 rays are walked in the order of a key
  * made of the direction's octant and a Morton code of the origin (a stable sort; lanes of a warp
- * then walk neighbouring rays), answers written back in the caller's order (default); 0 = rays are
- * taken as given.  Results do not depend on it.  pt_query_rays_static never reorders. */
-pt_status pt_query_order(int enabled);
+ * then walk neighbouring rays), answers written back in the caller's order; 0 = rays are taken as
+ * given; 2 = ordered only when the scene's walked arrays (nodes, triangle and sphere records) are
+ * larger than the device's L2, where the ordering's better locality pays for the sort (default).
+ * Other values are PT_INVALID_ARGUMENT.  Results do not depend on it.  pt_query_rays_static never
+ * reorders. */
+pt_status pt_query_order(int mode);
 
 /* Timing of the traversal kernel alone: launches > 0 records a pair of CUDA events around each
  * of the scene's next walk-kernel launches (a ring of `launches` pairs; 0 stops recording), and

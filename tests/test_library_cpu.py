@@ -182,7 +182,7 @@ def test_bench_samples_and_launch_counts():
     a = bench.random_indices(1 << 20, 1000, 7)
     assert len(a) == 1000 and len(np.unique(a)) == 1000 and (np.diff(a.astype(np.int64)) > 0).all()
     assert np.array_equal(a, bench.random_indices(1 << 20, 1000, 7)) and a.max() < (1 << 20)
-    assert bench.walk_launches_per_query(1 << 25) == 8 and bench.walk_launches_per_query(1000) == 1
+    assert bench.walk_launches_per_query(True) == 8 and bench.walk_launches_per_query(False) == 1
     args = bench.parse([])
     assert args.steps >= 1 and args.warmup >= 3 and args.parity_rays == 1 << 20 and args.log2_rays == 25
 

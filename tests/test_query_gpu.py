@@ -218,7 +218,7 @@ def test_ray_order_keeps_answers(oracle, layout):
             torch.cuda.synchronize()
             out[order] = (h.cpu().numpy(), a.cpu().numpy())
     finally:
-        pt.query_order(1)
+        pt.query_order(2)
     for x, y in zip(out[0], out[1]):
         assert x.tobytes() == y.tobytes()
     got = out[1][0].view(pt.HIT)
