@@ -158,7 +158,8 @@ __global__ void __launch_bounds__(256, 4) shade_kernel(DeviceScene scene, Render
 // finish: the queue's remaining paths run to the end of their pixel's samples, one thread per
 // path (the reference's megakernel form).  Used once the queue is short, where a wavefront
 // iteration would cost the latency of its slowest ray for a handful of rays, on two-wide trees,
-// with the brute-force walk and for the bvh / intersections views (otherwise finish_pair_kernel).
+// with the brute-force walk, for the bvh / intersections views and on trees of at most 32
+// four-wide nodes (otherwise finish_pair_kernel).
 __global__ void finish_kernel(DeviceScene scene, RenderParams p, RenderBuffers b, int parity) {
     const int32_t n = b.counters[parity];
     const bool reference_order = p.debug == PT_DEBUG_BVH || p.debug == PT_DEBUG_INTERSECTIONS;
@@ -366,6 +367,7 @@ struct pt_renderer {
     int block = 256;
     int grid_extend = 0, grid_shade = 0, grid_shadow = 0, grid_finish = 0, grid_finish_pair = 0;
     int32_t tail_paths = 0;             // live-path count below which the fused finish kernel takes over
+    bool pair_tail = false;             // the tail runs two lanes per path (finish_pair_kernel)
     DeviceBuffer paths, hits, stats, shadows, queue0, queue1, shadow_queue, counters, fetch, ray_total, error, sums, rng, rgba;
     RenderBuffers buf{};
     cudaStream_t stream = nullptr;
@@ -453,6 +455,12 @@ pt_status pt_renderer_create(const pt_scene *scene, const pt_camera *camera, int
             // below 65,536 live paths the fused kernel holds them all at once (measured: config 1 is 3.6 %
             // faster than with a floor of 16,384; larger images are unchanged)
             r->tail_paths = std::max<int32_t>(65536, r->pixels / 4);
+            // Two lanes per path pay when a walk costs more than the shading around it; on a tree of a
+            // few nodes (tens of primitives) the bounce is mostly shading and one lane per path is
+            // faster (measured: 23 primitives 7.1 vs 8.4 ms for config 1; 772 triangles 3.4 vs 4.1 ms
+            // the other way).
+            constexpr size_t kPairTailMinNodes = 32;
+            r->pair_tail = p.wide && scene->nodes4.bytes() / sizeof(Bvh4QNode) > kPairTailMinNodes;
         } catch (...) { delete r; throw; }
         *out = r;
         pt_status st = pt_reset(r, camera);
@@ -526,7 +534,7 @@ pt_status pt_add_samples(pt_renderer *r, int count) {
         if (tail && !done) {
             // the few remaining paths (of the last issued iteration's queue) run to completion
             const RenderParams &q = r->params;
-            if (q.wide && !q.brute && q.debug != PT_DEBUG_BVH && q.debug != PT_DEBUG_INTERSECTIONS) {
+            if (r->pair_tail && !q.brute && q.debug != PT_DEBUG_BVH && q.debug != PT_DEBUG_INTERSECTIONS) {
                 PT_CUDA(cudaMemsetAsync(&r->buf.fetch[3], 0, sizeof(unsigned long long), st));
                 finish_pair_kernel<<<r->grid_finish_pair, r->block, 0, st>>>(scene, q, r->buf, parity);
             } else

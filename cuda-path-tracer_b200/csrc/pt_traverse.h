@@ -882,11 +882,9 @@ __device__ inline void persistent_walk4_spec(const DeviceScene &s, size_t count,
         const int threshold = pool_empty ? 1 : min_active;
         for (;;) {
             bool end = false;
-            // ---- node phase
+            // ---- node phase: per iteration a node step, the postponement of a leaf, and at most one pop
             for (;;) {
-                if (busy && leaf == kNone && cur < 0) { leaf = cur; cur = pop(); }
-                bool searching = busy && leaf == kNone && cur != kNone;
-                if (!__any_sync(0xffffffffu, searching)) break;
+                bool need_pop = false;
                 if (busy && cur >= 0 && cur != kNone && !error) {
                     int32_t ref[4];
                     float dist[4];
@@ -905,9 +903,13 @@ __device__ inline void persistent_walk4_spec(const DeviceScene &s, size_t count,
                             cur = ref[0];
                         }
                     } else {
-                        cur = pop();
+                        need_pop = true;
                     }
                 }
+                if (busy && leaf == kNone && cur < 0) { leaf = cur; need_pop = true; }
+                if (need_pop) cur = pop();
+                bool searching = busy && leaf == kNone && cur != kNone;
+                if (!__any_sync(0xffffffffu, searching)) break;
             }
             // ---- leaf phase
             if (busy && leaf != kNone) {
