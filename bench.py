@@ -1048,7 +1048,7 @@ def main(argv=None):
         same = bool(h_hits.numpy().tobytes() == hits.cpu().numpy().tobytes())
         e2e = {"value": whole_job_rate(world, n, e_steps, e_dt) / 1e9, "unit": UNIT, "h2d_bytes_per_step": n * 28,
                "d2h_bytes_per_step": n * 16, "ms_per_step": e_dt / e_steps * 1e3,
-               "api": "pt_query_rays (host buffers, 3-stream chunked pipeline)", "hits_equal_device_path": same}
+               "api": "pt_query_rays (host buffers, chunks of 2^20 rays over 3 streams)", "hits_equal_device_path": same}
         del h_rays, h_hits
 
     # CPU baselines on the host cores (rank 0 at N=1)

@@ -132,7 +132,7 @@ __global__ void batch_start(BatchBuffers b, int32_t slots) {
 
 // kWide: four-wide nodes (phased walk) or the two-wide layout.
 template <bool kWide>
-__global__ void batch_extend(DeviceScene scene, BatchBuffers b, int parity, int min_active) {
+__global__ void __launch_bounds__(256, 4) batch_extend(DeviceScene scene, BatchBuffers b, int parity, int min_active) {
     const int32_t n = b.counters[parity];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         atomicAdd(b.rays, (unsigned long long)n);
@@ -206,7 +206,7 @@ __global__ void batch_shade(DeviceScene scene, BatchBuffers b, int parity) {
 }
 
 template <bool kWide>
-__global__ void batch_shadow(DeviceScene scene, BatchBuffers b, int parity, int min_active) {
+__global__ void __launch_bounds__(256, 4) batch_shadow(DeviceScene scene, BatchBuffers b, int parity, int min_active) {
     const int32_t n = b.counters[2 + parity];
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(b.rays, (unsigned long long)n);
     auto get = [&](size_t k, pt_ray &r, float &lo, float &hi, int32_t &root) {

@@ -159,7 +159,7 @@ __global__ void __launch_bounds__(256, 4) shade_kernel(DeviceScene scene, Render
 // path (the reference's megakernel form).  Used once the queue is short, where a wavefront
 // iteration would cost the latency of its slowest ray for a handful of rays, on two-wide trees,
 // with the brute-force walk, for the bvh / intersections views and on trees of at most 32
-// four-wide nodes (otherwise finish_pair_kernel).
+// four-wide nodes, which the renderer walks in the two-wide layout (otherwise finish_pair_kernel).
 __global__ void finish_kernel(DeviceScene scene, RenderParams p, RenderBuffers b, int parity) {
     const int32_t n = b.counters[parity];
     const bool reference_order = p.debug == PT_DEBUG_BVH || p.debug == PT_DEBUG_INTERSECTIONS;
@@ -455,12 +455,14 @@ pt_status pt_renderer_create(const pt_scene *scene, const pt_camera *camera, int
             // below 65,536 live paths the fused kernel holds them all at once (measured: config 1 is 3.6 %
             // faster than with a floor of 16,384; larger images are unchanged)
             r->tail_paths = std::max<int32_t>(65536, r->pixels / 4);
-            // Two lanes per path pay when a walk costs more than the shading around it; on a tree of a
-            // few nodes (tens of primitives) the bounce is mostly shading and one lane per path is
-            // faster (measured: 23 primitives 7.1 vs 8.4 ms for config 1; 772 triangles 3.4 vs 4.1 ms
-            // the other way).
-            constexpr size_t kPairTailMinNodes = 32;
-            r->pair_tail = p.wide && scene->nodes4.bytes() / sizeof(Bvh4QNode) > kPairTailMinNodes;
+            // On a tree of a few nodes (tens of primitives) a bounce is mostly shading: the two-wide walk
+            // (fewer instructions per visit) and one lane per path in the tail are faster there
+            // (config 1, 23 primitives: 8.4 ms per render with the four-wide walk and two lanes per
+            // path, 6.8 with one lane, 6.5 with the two-wide walk too); from a few hundred triangles on,
+            // two lanes per path win (772 triangles: 3.4 vs 4.1 ms).
+            constexpr size_t kSmallTreeNodes = 32;
+            if (p.wide && scene->nodes4.bytes() / sizeof(Bvh4QNode) <= kSmallTreeNodes) p.wide = 0;
+            r->pair_tail = p.wide != 0;
         } catch (...) { delete r; throw; }
         *out = r;
         pt_status st = pt_reset(r, camera);

@@ -814,10 +814,12 @@ __device__ inline void persistent_walk4(const DeviceScene &s, size_t count, unsi
 namespace ptb {
 
 // Four-wide walk in two phases per round (speculative while-while): in the node phase every
-// lane walks inner nodes until it holds one postponed leaf — lanes that already hold one keep
-// walking speculatively while others search — and in the leaf phase all lanes test their leaf
-// together, so node work and primitive work do not diverge inside one warp instruction
-// stream.  Same contract and answer as persistent_walk4.
+// lane walks inner nodes until it holds a postponed leaf — lanes that already hold one keep
+// walking speculatively while others search, and postpone a second leaf when they reach one —
+// and in the leaf phase all lanes test their leaves together, so node work and primitive work
+// do not diverge inside one warp instruction stream.  Same contract and answer as
+// persistent_walk4 (a leaf tested after a nearer hit was found only costs time: the triangle
+// tests take the current closest distance as their limit).
 // With kRoot, get() also returns the walk's root node (several trees in one node array; < 0 for
 // an empty tree).
 template <bool kAny, bool kRoot = false, class Get, class Done>
@@ -837,7 +839,7 @@ __device__ inline void persistent_walk4_spec(const DeviceScene &s, size_t count,
     long long best_key = 0;
     HitInfo hit;
     uint32_t boxes = 0, prims = 0;
-    int32_t cur = kNone, leaf = kNone;
+    int32_t cur = kNone, leaf = kNone, leaf2 = kNone;
     int sp = 0;
     bool found = false;
     int error = 0;
@@ -873,7 +875,7 @@ __device__ inline void persistent_walk4_spec(const DeviceScene &s, size_t count,
                     hit.slot = -1; hit.t = 0; hit.u = 0; hit.v = 0;
                     boxes = 0; prims = 0; sp = 0; found = false; error = 0;
                     cur = (s.empty || s.node_count == 0 || root < 0) ? kNone : root;
-                    leaf = kNone;
+                    leaf = kNone; leaf2 = kNone;
                     busy = true;
                 }
             }
@@ -890,7 +892,7 @@ __device__ inline void persistent_walk4_spec(const DeviceScene &s, size_t count,
                     float dist[4];
                     int hits = node4_children(s, cur, rb, tmin, limit, ref, dist, boxes);
                     if (hits) {
-                        if (sp + hits - 1 > kStack4) { error = 1; cur = kNone; leaf = kNone; }
+                        if (sp + hits - 1 > kStack4) { error = 1; cur = kNone; leaf = kNone; leaf2 = kNone; }
                         else {
 #pragma unroll
                             for (int k = 3; k >= 1; k--) {    // static indices: ref/dist stay in registers
@@ -906,7 +908,10 @@ __device__ inline void persistent_walk4_spec(const DeviceScene &s, size_t count,
                         need_pop = true;
                     }
                 }
-                if (busy && leaf == kNone && cur < 0) { leaf = cur; need_pop = true; }
+                if (busy && cur < 0) {
+                    if (leaf == kNone) { leaf = cur; need_pop = true; }
+                    else if (leaf2 == kNone) { leaf2 = cur; need_pop = true; }
+                }
                 if (need_pop) cur = pop();
                 bool searching = busy && leaf == kNone && cur != kNone;
                 if (!__any_sync(0xffffffffu, searching)) break;
@@ -917,6 +922,13 @@ __device__ inline void persistent_walk4_spec(const DeviceScene &s, size_t count,
                 else if (found) limit = nextafterf(closest, tmax);
                 leaf = kNone;
             }
+            if (busy && leaf2 != kNone) {
+                if (!(kAny && end)) {
+                    if (leaf4<kAny>(s, leaf2, r, dl, tmin, tmax, tie, found, closest, best_key, hit, prims) && kAny) end = true;
+                    else if (found) limit = nextafterf(closest, tmax);
+                }
+                leaf2 = kNone;
+            }
             if (busy && (end || error || (leaf == kNone && cur == kNone))) {
                 WalkResult res;
                 if (error) found = false;
@@ -924,7 +936,7 @@ __device__ inline void persistent_walk4_spec(const DeviceScene &s, size_t count,
                 res.boxes = boxes; res.prims = prims; res.error = error;
                 done(index, res);
                 busy = false;
-                cur = kNone; leaf = kNone;
+                cur = kNone; leaf = kNone; leaf2 = kNone;
             }
             if (__popc(__ballot_sync(0xffffffffu, busy)) < threshold) break;
         }
