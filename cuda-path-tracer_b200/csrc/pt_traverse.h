@@ -918,16 +918,17 @@ __device__ inline void persistent_walk4_spec(const DeviceScene &s, size_t count,
             }
             // ---- leaf phase
             if (busy && leaf != kNone) {
-                if (leaf4<kAny>(s, leaf, r, dl, tmin, tmax, tie, found, closest, best_key, hit, prims) && kAny) end = true;
-                else if (found) limit = nextafterf(closest, tmax);
-                leaf = kNone;
-            }
-            if (busy && leaf2 != kNone) {
-                if (!(kAny && end)) {
-                    if (leaf4<kAny>(s, leaf2, r, dl, tmin, tmax, tie, found, closest, best_key, hit, prims) && kAny) end = true;
-                    else if (found) limit = nextafterf(closest, tmax);
+                // both postponed leaves' slots in one loop (a lane with one short leaf does not wait
+                // for the warp's longest first leaf and then its longest second one)
+                const int32_t v1 = ~leaf, f1 = v1 >> 3, c1 = (v1 & 7) + 1;
+                int32_t f2 = 0, c2 = 0;
+                if (leaf2 != kNone) { const int32_t v2 = ~leaf2; f2 = v2 >> 3; c2 = (v2 & 7) + 1; }
+                for (int32_t j = 0; j < c1 + c2; j++) {
+                    const int32_t slot = j < c1 ? f1 + j : f2 + (j - c1);
+                    if (test_leaf<kAny>(s, slot, r, dl, tmin, tmax, tie, found, closest, best_key, hit, prims) && kAny) { end = true; break; }
                 }
-                leaf2 = kNone;
+                if (!end && found) limit = nextafterf(closest, tmax);
+                leaf = kNone; leaf2 = kNone;
             }
             if (busy && (end || error || (leaf == kNone && cur == kNone))) {
                 WalkResult res;
