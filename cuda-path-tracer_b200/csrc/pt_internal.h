@@ -57,10 +57,10 @@ constexpr int kLeafMax = 4;   // slots per four-wide leaf
 // steps covering the union.  An empty slot has its lower bounds above its upper ones.
 struct alignas(64) Bvh4QNode {
     float px, py, pz;
-    uint32_t exps;                 // biased exponents of the grid spacing: x | y << 8 | z << 16
+    float sx;                      // grid spacing along x (a power of two)
     uint32_t qlo[3], qhi[3];       // per axis; child k in byte k
     int32_t child[4];
-    uint32_t pad[2];
+    float sy, sz;                  // grid spacings along y and z
 };
 static_assert(sizeof(Bvh4QNode) == 64, "quantized four-wide node is 64 bytes");
 

@@ -269,7 +269,7 @@ Bvh4QNode quantize4(const Bvh4Node &n) {
         if(n.child[k] == kEmptyChild) continue;
         for(int a = 0; a < 3; a++) { lo[a] = std::min(lo[a], double(L[a][k])); hi[a] = std::max(hi[a], double(H[a][k])); }
     }
-    float *P[3] = {&q.px, &q.py, &q.pz};
+    float *P[3] = {&q.px, &q.py, &q.pz}, *S[3] = {&q.sx, &q.sy, &q.sz};
     for(int a = 0; a < 3; a++) {
         if(!(lo[a] <= hi[a])) { lo[a] = hi[a] = 0; }
         *P[a] = float(lo[a]);
@@ -278,7 +278,7 @@ Bvh4QNode quantize4(const Bvh4Node &n) {
         while(std::ldexp(255.0, e) < ext) e++;
         e = std::max(-126, std::min(127, e));
         const double step = std::ldexp(1.0, e);
-        q.exps |= uint32_t(e + 127) << (8 * a);
+        *S[a] = float(step);
         for(int k = 0; k < 4; k++) {
             uint32_t ql = 255, qh = 0;   // an empty slot: inverted
             if(n.child[k] != kEmptyChild) {

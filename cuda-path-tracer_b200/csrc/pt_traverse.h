@@ -581,7 +581,7 @@ PT_HD inline void load_node4(const DeviceScene &s, int32_t node, Bvh4QNode &n) {
     float x[8], y[8];
     ldg8(p, x);
     ldg8(p + 8, y);
-    n.px = x[0]; n.py = x[1]; n.pz = x[2]; n.exps = __float_as_uint(x[3]);
+    n.px = x[0]; n.py = x[1]; n.pz = x[2]; n.sx = x[3]; n.sy = y[6]; n.sz = y[7];
     n.qlo[0] = __float_as_uint(x[4]); n.qlo[1] = __float_as_uint(x[5]); n.qlo[2] = __float_as_uint(x[6]);
     n.qhi[0] = __float_as_uint(x[7]); n.qhi[1] = __float_as_uint(y[0]); n.qhi[2] = __float_as_uint(y[1]);
     n.child[0] = __float_as_int(y[2]); n.child[1] = __float_as_int(y[3]); n.child[2] = __float_as_int(y[4]); n.child[3] = __float_as_int(y[5]);
@@ -590,19 +590,12 @@ PT_HD inline void load_node4(const DeviceScene &s, int32_t node, Bvh4QNode &n) {
 #endif
 }
 
-// byte k of w as a float, exactly: the byte placed in the mantissa of 2^23, then 2^23 subtracted
+// byte k of w as a float, exactly (one integer-to-float conversion of the byte on the device)
 PT_HD inline float qbyte(uint32_t w, int k) {
 #ifdef __CUDA_ARCH__
-    return __int_as_float(int(__byte_perm(w, 0x4b000000u, 0x7540u + unsigned(k)))) - 8388608.0f;
+    return __uint2float_rn((w >> (8 * k)) & 0xffu);
 #else
     return float((w >> (8 * k)) & 0xffu);
-#endif
-}
-PT_HD inline float exp2_of(uint32_t biased) {
-#ifdef __CUDA_ARCH__
-    return __int_as_float(int(biased << 23));
-#else
-    uint32_t bits = biased << 23; float f; std::memcpy(&f, &bits, 4); return f;
 #endif
 }
 
@@ -611,7 +604,7 @@ PT_HD inline int node4_children(const DeviceScene &s, int32_t node, const RayBox
                                 int32_t ref[4], float dist[4], uint32_t &boxes) {
     Bvh4QNode n;
     load_node4(s, node, n);
-    const float sx = exp2_of(n.exps & 0xffu) * rb.jx, sy = exp2_of((n.exps >> 8) & 0xffu) * rb.jy, sz = exp2_of((n.exps >> 16) & 0xffu) * rb.jz;
+    const float sx = n.sx * rb.jx, sy = n.sy * rb.jy, sz = n.sz * rb.jz;
     const float tx = fma_box(n.px, rb.jx, rb.kx), ty = fma_box(n.py, rb.jy, rb.ky), tz = fma_box(n.pz, rb.jz, rb.kz);
     const uint32_t nxw = rb.nx ? n.qhi[0] : n.qlo[0], fxw = rb.nx ? n.qlo[0] : n.qhi[0];
     const uint32_t nyw = rb.ny ? n.qhi[1] : n.qlo[1], fyw = rb.ny ? n.qlo[1] : n.qhi[1];
