@@ -385,7 +385,8 @@ def roofline_record(bytes_per_ray, n, walk_ms, hbm, l2_gbs, traffic, kind, extra
 def reference_gpu_record(scene, dev, rays_u8, n, value_grays, compat_rays: int = 1 << 20):
     """The reference's own query_rays kernel on the same device-resident rays (same GPU), and
     pt_query_rays_compat against its cuda_query_rays, bytewise, on a slice of `compat_rays` rays
-    (the first half of them camera rays, the second half bounce rays)."""
+    (the first half of them from the batch's first half, camera rays; the rest from its second half,
+    bounce rays for config 2 and surface rays for config 3)."""
     sys.path.insert(0, str(ROOT / "oracle"))
     from oracle_bind import RefGpuTiming, RefGpu, REF_TIMING_SO, REF_GPU_SO
     if not REF_TIMING_SO.exists() or not REF_GPU_SO.exists():
@@ -498,6 +499,9 @@ def c3_record(args, hbm, l2_gbs, kind, check_rays: int = 1 << 16):
                                                                           "primitive counts; the reference's depth-first walk "
                                                                           "tests about twice as many boxes, which is why the "
                                                                           "fraction above can exceed 1"}})}
+    # the reference's own query kernel on the same rays (and its cuda_query_rays on a slice)
+    out["closest"]["reference_gpu"] = guarded("c3 reference_gpu", reference_gpu_record, scene, dev, rays, n,
+                                              out["closest"]["value"], compat_rays=1 << 18)
     # any hit: shadow rays between surface points
     tmax = torch.empty(n * 4, dtype=torch.uint8, device="cuda")
     dev.surface_rays_device(5, 0, n, rays, tmax=tmax)
@@ -866,7 +870,8 @@ def render_record(args, dev=None, scene=None, cam=None, steps: int = 3, warmup: 
                   workload: str = "progressive render of the procedural 1M-triangle scene, 960x600, 64 spp, bounce limit 8, MIS"):
     """The progressive renderer (one step = a full render from a reset; by default the procedural
     1M-triangle scene, 960x600, 64 spp, bounce limit 8, MIS) beside the reference's own CUDA
-    renderer built with its bounce limit set to D ("patched reference", oracle/_ref) on the same
+    renderer built with its bounce limit set to D ("patched reference", oracle/_ref; D = 50 is the
+    reference's own limit, its unpatched build) on the same
     GPU: Mrays/s = rays traced / kernel time, as the reference reports it
     (src/cuda/cuda_renderer.cu:196-213, 246-247), and the two images compared bitwise."""
     t = time.perf_counter()
@@ -893,8 +898,9 @@ def render_record(args, dev=None, scene=None, cam=None, steps: int = 3, warmup: 
     ref_line = None
     sys.path.insert(0, str(ROOT / "oracle"))
     from oracle_bind import RefGpu, ref_gpu_so, RefCpu, REF_CPU_SO
-    if ref_gpu_so(D).exists():
-        gpu = RefGpu(D)
+    unpatched = D == 50                        # the reference's own bounce limit: its stock build
+    if ref_gpu_so(None if unpatched else D).exists():
+        gpu = RefGpu(None if unpatched else D)
         rr = gpu.renderer(scene, cam, W, H, 1, mis=True)
         rr.add_samples(SPP)                    # warm-up render
         rr.close()
@@ -909,7 +915,8 @@ def render_record(args, dev=None, scene=None, cam=None, steps: int = 3, warmup: 
             same = same and rr.image().tobytes() == img.tobytes()
             rr.close()
         ref_line = {"mrays_per_s": rrays / rms / 1e3, "ms_per_render": rms / steps,
-                    "kind": "reference cuda_renderer, bounce limit 8 (patched reference), same GPU",
+                    "kind": ("reference cuda_renderer, unpatched (its own bounce limit 50), same GPU" if unpatched else
+                             f"reference cuda_renderer, bounce limit {D} (patched reference), same GPU"),
                     "images_bit_identical": bool(same), "rays_equal": bool(rrays == rays),
                     "speedup": value / (rrays / rms / 1e3)}
     cpu_rec = None
@@ -1107,6 +1114,9 @@ def main(argv=None):
     torch.cuda.empty_cache()
     if extras and not args.no_render:
         line["render_c2"] = guarded("render_c2", render_record, args, dev=dev, scene=scene, cam=cam)
+        line["render_c2_depth50"] = guarded("render_c2_depth50", render_record, args, dev=dev, scene=scene, cam=cam, steps=2, D=50,
+                                            workload="progressive render of the procedural 1M-triangle scene, 960x600, 64 spp, "
+                                                     "bounce limit 50 (the reference's own), MIS")
         cornell, ccam = pt.cornell_box(320, 200)
         line["render_c1"] = guarded("render_c1", render_record, args, dev=pt.Scene(cornell), scene=cornell, cam=ccam, steps=5,
                                     warmup=2, W=320, H=200, SPP=16, D=8, cpu=True,
