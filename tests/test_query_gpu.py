@@ -228,6 +228,26 @@ def test_ray_order_keeps_answers(oracle, layout):
     assert_hits_equal(got[pick], oracle.query(s, host[pick]))
 
 
+def test_ray_order_modes():
+    """pt_query_order: 0 never orders, 1 orders batches of at least 2^18 rays, 2 (the default) only
+    on scenes whose walked arrays exceed the L2 (a small scene: not ordered); other modes are
+    rejected and leave the setting as it was."""
+    s, _ = pt.procedural_scene(64, 64, sphere_count=2, segments=32, rings=17, seed=3)
+    dev = pt.Scene(s)
+    try:
+        assert not dev.query_ordered(1 << 20)                # default mode 2, scene far below the L2
+        pt.query_order(1)
+        assert dev.query_ordered(1 << 18) and not dev.query_ordered((1 << 18) - 1)
+        with pytest.raises(pt.PtError) as e:
+            pt.query_order(3)
+        assert e.value.status == 1                           # PT_INVALID_ARGUMENT
+        assert dev.query_ordered(1 << 18)                    # still mode 1
+        pt.query_order(0)
+        assert not dev.query_ordered(1 << 20)
+    finally:
+        pt.query_order(2)
+
+
 def _sample_rows(dev_u8, idx, width, dtype):
     import torch
     return dev_u8.view(-1, width)[torch.from_numpy(idx.astype(np.int64)).cuda()].cpu().numpy().view(dtype).reshape(-1)
