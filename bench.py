@@ -77,6 +77,9 @@ def parse(argv=None):
                          "one launch; cache: radiance-cache renderer vs plain at 1920x1080; render: config-2 renderer "
                          "vs the reference's; c3: the 9.4M-triangle traversal microbenchmark")
     ap.add_argument("--jobs", type=int, default=48)
+    ap.add_argument("--render-scene", choices=["procedural", "cornell"], default="procedural",
+                    help="render workload: config 2 (procedural 1M triangles, 960x600, 64 spp) or config 1 (Cornell "
+                         "box, 320x200, 16 spp), bounce limit 8")
     ap.add_argument("--ref-spp", type=int, default=65536,
                     help="cache workload: samples of the FP64 reference image (0: time cached frames only)")
     ap.add_argument("--max-spp", type=int, default=4096, help="cache workload: sample budget of each curve")
@@ -939,15 +942,24 @@ def run_render(args):
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     clocks = Clocks(local)
-    rec = render_record(args, steps=max(1, args.steps), warmup=max(1, args.warmup), cpu=not args.no_cpu_baseline)
+    if args.render_scene == "cornell":
+        cornell, ccam = pt.cornell_box(320, 200)
+        rec = render_record(args, dev=pt.Scene(cornell), scene=cornell, cam=ccam, steps=max(1, args.steps),
+                            warmup=max(1, args.warmup), W=320, H=200, SPP=16, D=8, cpu=not args.no_cpu_baseline,
+                            workload="Cornell box (20 triangles, 3 spheres), 320x200, 16 spp, bounce limit 8, MIS, seed 1")
+        metric = "Mrays/s render (Cornell box, 320x200, 16 spp, depth 8, MIS)"
+    else:
+        rec = render_record(args, steps=max(1, args.steps), warmup=max(1, args.warmup), cpu=not args.no_cpu_baseline)
+        metric = "Mrays/s render (procedural 1M, 960x600, 64 spp, depth 8, MIS)"
     clock = clocks.stop()
-    line = {"metric": "Mrays/s render (procedural 1M, 960x600, 64 spp, depth 8, MIS)", "value": rec["mrays_per_s"],
+    line = {"metric": metric, "value": rec["mrays_per_s"],
             "unit": "Mrays/s", "n_gpus": 1, "steps": rec["steps"], "warmup": max(1, args.warmup),
             "ms_per_step": rec["ms_per_render"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic", "config": {"workload": rec["workload"], "l2": "frame state > L2"},
-            "render_c2": rec, "clocks": clock,
+            ("render_c1" if args.render_scene == "cornell" else "render_c2"): rec, "clocks": clock,
             "e2e": {"value": rec["e2e_mrays_per_s"], "unit": "Mrays/s", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 960 * 600 * 12, "api": "pt_add_samples + pt_get_image (host wall clock)"},
+                    "d2h_bytes_per_step": (320 * 200 if args.render_scene == "cornell" else 960 * 600) * 12,
+                    "api": "pt_add_samples + pt_get_image (host wall clock)"},
             "cpu_baseline": rec["cpu_baseline"]}
     print(json.dumps(line), flush=True)
 
