@@ -160,6 +160,24 @@ __global__ void __launch_bounds__(256, 4) shade_kernel(DeviceScene scene, Render
 // iteration would cost the latency of its slowest ray for a handful of rays, on two-wide trees,
 // with the brute-force walk, for the bvh / intersections views and on trees of at most 32
 // four-wide nodes, which the renderer walks in the two-wide layout (otherwise finish_pair_kernel).
+// walk forms the one-lane finish kernel rarely runs (brute force, the debug views' reference-order
+// walk, four-wide trees outside the pair tail), called out of line so that the bounce loop's hot
+// path stays compact in the instruction cache
+template <bool kAny>
+__device__ __noinline__ bool cold_brute(const DeviceScene &scene, const int32_t *order, int32_t leaves, const pt_ray &r, float tmax,
+                                        HitInfo &h, uint32_t &prims) {
+    return traverse_brute<kAny>(scene, order, leaves, r, 0.001f, tmax, kTieLastNode, h, prims);
+}
+__device__ __noinline__ bool cold_reference(const DeviceScene &scene, const pt_ray &r, HitInfo &h, uint32_t &boxes, uint32_t &prims,
+                                            int &error) {
+    return traverse_reference(scene, r, 0.001f, FLT_MAX, kTieLastLeaf, h, boxes, prims, error);
+}
+template <bool kAny>
+__device__ __noinline__ bool cold_walk4(const DeviceScene &scene, const pt_ray &r, float tmax, HitInfo &h, uint32_t &boxes,
+                                        uint32_t &prims, int &error) {
+    return traverse4<kAny>(scene, r, 0.001f, tmax, kTieLastLeaf, h, boxes, prims, error);
+}
+
 __global__ void finish_kernel(DeviceScene scene, RenderParams p, RenderBuffers b, int parity) {
     const int32_t n = b.counters[parity];
     const bool reference_order = p.debug == PT_DEBUG_BVH || p.debug == PT_DEBUG_INTERSECTIONS;
@@ -175,9 +193,9 @@ __global__ void finish_kernel(DeviceScene scene, RenderParams p, RenderBuffers b
             uint32_t boxes = 0, prims = 0;
             int error = 0;
             bool hit;
-            if (p.brute) hit = traverse_brute<false>(scene, p.brute_order, p.leaves, r, 0.001f, FLT_MAX, kTieLastNode, hi, prims);
-            else if (reference_order) hit = traverse_reference(scene, r, 0.001f, FLT_MAX, kTieLastLeaf, hi, boxes, prims, error);
-            else if (p.wide) hit = traverse4<false>(scene, r, 0.001f, FLT_MAX, kTieLastLeaf, hi, boxes, prims, error);
+            if (p.brute) hit = cold_brute<false>(scene, p.brute_order, p.leaves, r, FLT_MAX, hi, prims);
+            else if (reference_order) hit = cold_reference(scene, r, hi, boxes, prims, error);
+            else if (p.wide) hit = cold_walk4<false>(scene, r, FLT_MAX, hi, boxes, prims, error);
             else hit = traverse<false>(scene, r, 0.001f, FLT_MAX, kTieLastLeaf, hi, boxes, prims, error);
             if (error) *b.error = 1;
             PathHit h;
@@ -194,8 +212,8 @@ __global__ void finish_kernel(DeviceScene scene, RenderParams p, RenderBuffers b
                 HitInfo sh;
                 uint32_t sb = 0, spr = 0;
                 int serr = 0;
-                bool blocked = p.brute ? traverse_brute<true>(scene, p.brute_order, p.leaves, q, 0.001f, sr.tmax, kTieLastNode, sh, spr)
-                             : p.wide ? traverse4<true>(scene, q, 0.001f, sr.tmax, kTieLastLeaf, sh, sb, spr, serr)
+                bool blocked = p.brute ? cold_brute<true>(scene, p.brute_order, p.leaves, q, sr.tmax, sh, spr)
+                             : p.wide ? cold_walk4<true>(scene, q, sr.tmax, sh, sb, spr, serr)
                                       : traverse<true>(scene, q, 0.001f, sr.tmax, kTieLastLeaf, sh, sb, spr, serr);
                 if (serr) *b.error = 1;
                 else if (!blocked) { s.rr = s.rr + sr.cr; s.rg = s.rg + sr.cg; s.rb = s.rb + sr.cb; }
