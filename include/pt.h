@@ -180,7 +180,9 @@ pt_status pt_query_rays_brute_device(const pt_scene *scene, const pt_ray *rays, 
 pt_status pt_query_tuning(int persistent, int min_active, int blocks_per_sm);
 /* Node layout of the traversal kernels (process-wide; renderers pick it up when created):
  * 1 = four-wide nodes (up to 4 primitives per leaf) where the scene's tree allows it (default),
- * 0 = the two-wide re-layout of the caller's tree.  Results do not depend on it. */
+ * 0 = the two-wide re-layout of the caller's tree.  A renderer of a tree of at most 32 four-wide
+ * nodes walks the two-wide layout either way (faster on so few nodes).  Results do not depend
+ * on it. */
 pt_status pt_query_layout(int wide);
 /* Four-wide walk form (process-wide): 1 = separate node and leaf phases per warp round, lanes
  * that already hold a leaf walking on speculatively (default); 0 = nodes and leaves in one loop. */
