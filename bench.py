@@ -691,7 +691,7 @@ def cache_record(args, diffuse_only=True, cpu=True):
     """Radiance cache vs plain path tracing on the procedural 1M-triangle scene at 1920x1080,
     depth 12, MIS: relMSE-vs-time curves against an FP64-accumulated plain reference, the time
     each method needs to reach the plain method's 1024-spp relMSE and relMSE <= 1e-3, in wall time
-    (host clock around the render calls, the north star's measure) and device time (CUDA events)."""
+    (host clock around the render calls, the measure the target is stated in) and device time (CUDA events)."""
     W, H, D = 1920, 1080, 12
     t = time.perf_counter()
     scene, cam = pt.procedural_scene(W, H)
@@ -793,7 +793,7 @@ def cache_record(args, diffuse_only=True, cpu=True):
                                  f"= {rays / dt / 1e6:.1f} Mrays/s; value = plain rays to relMSE 1e-3 at that rate"}
     return {
         "workload": "radiance cache vs plain, procedural 1M-triangle scene, 1920x1080, depth 12, MIS",
-        "target": "the plain method's 1024-spp relMSE, reached in >= 4x less wall time (north-star target); "
+        "target": "the plain method's 1024-spp relMSE, reached in >= 4x less wall time (the stated target); "
                   "relMSE <= 1e-3 reported beside it",
         "wall_ms": {"cache_to_plain_1024": c_1024_wall, "plain_1024": plain_1024[3], "cache_to_1e-3": c_1e3_wall,
                     "plain_to_1e-3": p_1e3_wall},

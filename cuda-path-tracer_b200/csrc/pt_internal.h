@@ -98,7 +98,7 @@ struct DeviceScene {
     int32_t root_leaf;              // flat root is itself a leaf (no branch above it)
 };
 
-// Tie rule for exact-distance hits: the lowest (type, id) (north-star rule), the leaf the
+// Tie rule for exact-distance hits: the lowest (type, id) (the parity rule of the query API), the leaf the
 // reference's depth-first walk reaches last (trace_world, src/renderer/transport.h:76-79), or
 // the last leaf in node-array order (its brute-force scan, transport.h:48-60).
 enum TieRule : int { kTieLowestId = 0, kTieLastLeaf = 1, kTieLastNode = 2 };

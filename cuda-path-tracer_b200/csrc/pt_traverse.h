@@ -10,7 +10,7 @@
 // other pushed, and leaves are tested as soon as their box passes.  Because every
 // candidate's t is computed bit-identically and boxes are conservative, the set of
 // primitives at the closest distance is independent of the order; among them the winner is
-// picked by a key: the lowest (type, id) (the north-star rule) or, for the compatibility
+// picked by a key: the lowest (type, id) (the query API's rule) or, for the compatibility
 // entry point, the last depth-first leaf (the reference's rule, transport.h:76-79).
 #pragma once
 

@@ -1,6 +1,6 @@
 """GPU parity of the closest-hit / any-hit kernels against the oracle and the reference.
 
-Bar (north star): the same hit primitive as the reference's traversal, exact-distance ties
+Bar: the same hit primitive as the reference's traversal, exact-distance ties
 resolved to the lowest (type, id), and t within 1e-6 relative.  The kernels reproduce the
 reference's FP32 arithmetic, so these tests demand bit equality of t, which is stricter.
 """
@@ -16,7 +16,7 @@ from oracle_bind import Oracle, RefCpu, RefGpu, REF_CPU_SO, REF_GPU_SO
 
 pytestmark = pytest.mark.gpu
 G = np.load(Path(__file__).parent / "golden" / "reference_golden.npz")
-T_REL = 1e-6   # north-star tolerance on t (the checks below are bitwise, which implies it)
+T_REL = 1e-6   # tolerance on t (the checks below are bitwise, which implies it)
 
 
 def golden_scene(prefix):
@@ -104,7 +104,7 @@ def test_tmax_and_stats(oracle, layout):
 
 def test_exact_tie_lowest_id(layout):
     """transport_tests' pruning scene (tests/transport_tests.cpp:54-78): two coincident spheres.
-    The reference keeps the later leaf (material 1); the north-star rule keeps the lowest id."""
+    The reference keeps the later leaf (material 1); the query API's rule keeps the lowest id."""
     spheres = np.zeros(3, pt.SPHERE)
     spheres[0] = ((0, 0, 0), 1, 0)
     spheres[1] = ((0, 0, 0), 1, 1)
