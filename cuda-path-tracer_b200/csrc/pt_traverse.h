@@ -907,7 +907,11 @@ __device__ inline void persistent_walk4_spec(const DeviceScene &s, size_t count,
                 }
                 if (need_pop) cur = pop();
                 bool searching = busy && leaf == kNone && cur != kNone;
-                if (!__any_sync(0xffffffffu, searching)) break;
+                const unsigned sm = __ballot_sync(0xffffffffu, searching);
+                if (!sm) break;
+                // a few searching lanes do not hold the warp in the node phase once others have a
+                // leaf to test (the leaf phase then makes progress, so no round is empty)
+                if (__popc(sm) < 4 && __any_sync(0xffffffffu, busy && leaf != kNone)) break;
             }
             // ---- leaf phase
             if (busy && leaf != kNone) {
