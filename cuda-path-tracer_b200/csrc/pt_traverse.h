@@ -808,9 +808,10 @@ namespace ptb {
 
 // Four-wide walk in two phases per round (speculative while-while): in the node phase every
 // lane walks inner nodes until it holds a postponed leaf — lanes that already hold one keep
-// walking speculatively while others search, and postpone a second leaf when they reach one —
-// and in the leaf phase all lanes test their leaves together, so node work and primitive work
-// do not diverge inside one warp instruction stream.  Same contract and answer as
+// walking speculatively while others search, and postpone a second leaf when they reach one;
+// the phase also ends once fewer than four lanes are still searching while another holds a
+// leaf — and in the leaf phase all lanes test their leaves together, so node work and primitive
+// work do not diverge inside one warp instruction stream.  Same contract and answer as
 // persistent_walk4 (a leaf tested after a nearer hit was found only costs time: the triangle
 // tests take the current closest distance as their limit).
 // With kRoot, get() also returns the walk's root node (several trees in one node array; < 0 for
