@@ -140,8 +140,10 @@ enum { PT_QUERY_CLOSEST = 0, PT_QUERY_ANY = 1 };
 pt_status pt_query_rays_device(const pt_scene *scene, const pt_ray *rays, size_t count, int mode,
                                float tmin, const float *tmax, pt_hit *hits, pt_ray_stats *stats,
                                void *stream);
-/* Host buffers: uploads, traces and downloads in overlapped chunks; returns when `hits` is filled.
- * Calls on one scene from several host threads take turns (the staging buffers are the scene's). */
+/* Host buffers: uploads, traces and downloads in overlapped chunks (2^20 rays each, on three
+ * streams; the copies overlap the walk only from pinned host memory); returns when `hits` is
+ * filled.  Calls on one scene from several host threads take turns (the staging buffers are the
+ * scene's). */
 pt_status pt_query_rays(const pt_scene *scene, const pt_ray *rays, size_t count, int mode,
                         float tmin, const float *tmax, pt_hit *hits, pt_ray_stats *stats);
 /* Host-buffer query that allocates nothing.  Some callers cannot let a library call cudaMalloc
