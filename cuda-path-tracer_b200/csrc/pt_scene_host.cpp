@@ -5,6 +5,7 @@
 #include <functional>
 #include <thread>
 #include "pt_exact.h"
+#include "pt_api_common.h"
 #include "pt_host.h"
 
 namespace ptb {
@@ -407,3 +408,37 @@ HostLayout relayout(const pt_scene_desc &s) {
 }
 
 } // namespace ptb
+
+extern "C" {
+
+// Host-side check of the four-wide tree a scene would be walked with: rebuilds the re-layout as
+// pt_scene_create does and, in exact (double) arithmetic, checks every child's dequantised bounds
+// (origin + q * spacing) against the float bounds they stand for, and that empty slots are
+// inverted on every axis.
+pt_status pt_layout_check(const pt_scene_desc *desc, size_t *nodes, size_t *violations) {
+    return ptb::guard([&]() {
+        if(!desc || !nodes || !violations) throw ptb::Error(PT_INVALID_ARGUMENT, "null argument");
+        ptb::validate_scene(*desc);
+        const ptb::HostLayout layout = ptb::relayout(*desc);
+        size_t bad = 0;
+        for(size_t i = 0; i < layout.nodes4q.size(); i++) {
+            const ptb::Bvh4Node &f = layout.nodes4[i];
+            const ptb::Bvh4QNode &q = layout.nodes4q[i];
+            const float *L[3] = {f.lox, f.loy, f.loz}, *H[3] = {f.hix, f.hiy, f.hiz};
+            const double P[3] = {q.px, q.py, q.pz}, S[3] = {q.sx, q.sy, q.sz};
+            for(int k = 0; k < 4; k++) {
+                for(int a = 0; a < 3; a++) {
+                    const uint32_t lo = (q.qlo[a] >> (8 * k)) & 0xffu, hi = (q.qhi[a] >> (8 * k)) & 0xffu;
+                    if(q.child[k] != f.child[k]) { bad++; continue; }
+                    if(f.child[k] == ptb::kEmptyChild) { bad += !(lo > hi); continue; }
+                    bad += !(P[a] + lo * S[a] <= double(L[a][k]));
+                    bad += !(P[a] + hi * S[a] >= double(H[a][k]));
+                }
+            }
+        }
+        *nodes = layout.nodes4q.size();
+        *violations = bad;
+    });
+}
+
+} // extern "C"

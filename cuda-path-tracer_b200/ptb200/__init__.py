@@ -112,6 +112,7 @@ def library() -> C.CDLL:
         "pt_scene_lights": (I, [P, P, S, P, P]),
         "pt_scene_device_bytes": (I, [P, P]),
         "pt_query_ordered": (I, [P, S, P]),
+        "pt_layout_check": (I, [P, P, P]),
         "pt_query_rays_device": (I, [P, P, S, I, F, P, P, P, P]),
         "pt_query_rays_brute_device": (I, [P, P, S, I, F, P, P, P, P]),
         "pt_query_rays": (I, [P, P, S, I, F, P, P, P]),
@@ -316,6 +317,14 @@ def procedural_params(**overrides) -> ProceduralParams:
     for k, v in overrides.items():
         setattr(p, k, v)
     return p
+
+
+def layout_check(flat: "FlatScene") -> tuple[int, int]:
+    """(four-wide nodes, violations) of the tree pt_scene_create would build (pt_layout_check; host only)."""
+    d = flat.desc()
+    nodes, bad = C.c_size_t(), C.c_size_t()
+    check(library().pt_layout_check(C.byref(d), C.byref(nodes), C.byref(bad)))
+    return nodes.value, bad.value
 
 
 def procedural_scene(width: int = 960, height: int = 600, **overrides) -> tuple[FlatScene, np.ndarray]:

@@ -123,6 +123,11 @@ pt_status pt_scene_destroy(pt_scene *scene);
 pt_status pt_scene_lights(const pt_scene *scene, pt_light *lights, size_t capacity, size_t *count, float *total_area);
 /* Device bytes held by the scene (nodes, triangles, shading records, lights). */
 pt_status pt_scene_device_bytes(const pt_scene *scene, size_t *bytes);
+/* Host-side check of the four-wide tree pt_scene_create would build for `desc` (no device needed):
+ * *nodes = its node count (0 when the scene keeps the two-wide layout), *violations = child
+ * bounds whose 8-bit quantised form does not contain the float bounds, plus empty slots that are
+ * not inverted (0 for a correct build). */
+pt_status pt_layout_check(const pt_scene_desc *desc, size_t *nodes, size_t *violations);
 /* Whether a query of `count` rays on this scene is walked in key order under the current
  * pt_query_order setting (*ordered = 1: a key kernel and a radix sort run before the walk). */
 pt_status pt_query_ordered(const pt_scene *scene, size_t count, int *ordered);

@@ -115,6 +115,21 @@ def test_sah_builder_output_is_valid_and_keeps_ids():
     assert oracle.validate(again)
 
 
+def test_quantised_four_wide_tree_contains_every_child_box():
+    """The walked four-wide nodes hold each child's box as 8-bit bounds on a power-of-two grid:
+    the dequantised box must contain the float box it stands for (the box tests are conservative
+    filters only then), and empty slots must be inverted.  Checked on the host for a displaced-
+    sphere scene with a triangle soup, a scene with spheres and the Cornell box."""
+    scenes = [pt.procedural_scene(96, 60, sphere_count=4, segments=64, rings=33, seed=5, random_triangles=3000,
+                                  soup_edge_min=1e-3, soup_edge_max=1e-2)[0],
+              pt.procedural_scene(96, 60, sphere_count=2, segments=16, rings=9, seed=2, box_size=1000.0,
+                                  radius_min=1.0, radius_max=40.0)[0],
+              pt.cornell_box(64, 40)[0]]
+    for s in scenes:
+        nodes, bad = pt.layout_check(s)
+        assert nodes > 0 and bad == 0, (nodes, bad)
+
+
 def test_procedural_scene_counts():
     """The 1M-triangle scene: 16 spheres of 2*256*128 = 65,536 triangles, floor and light quads."""
     p = pt.procedural_params()
