@@ -130,6 +130,27 @@ def test_quantised_four_wide_tree_contains_every_child_box():
         assert nodes > 0 and bad == 0, (nodes, bad)
 
 
+def test_quantised_tree_is_conservative_at_extreme_scales():
+    """The quantised child bounds stay conservative far from the origin (coordinates near 1e5),
+    for tiny geometry (a 1e-4 scale), and with a degenerate (zero-area) triangle in the scene."""
+    base, _ = pt.procedural_scene(64, 40, sphere_count=3, segments=24, rings=13, seed=4, random_triangles=400)
+    cases = []
+    for scale, shift in ((1.0e1, 1.0e5), (1.0e-4, 0.0), (1.0, -3.0e3)):
+        s = base.copy()
+        for f in ("v0", "v1", "v2"):
+            s.triangles[f] = s.triangles[f] * np.float32(scale) + np.float32(shift)
+        s.spheres["center"] = s.spheres["center"] * np.float32(scale) + np.float32(shift)
+        s.spheres["radius"] = s.spheres["radius"] * np.float32(scale)
+        cases.append(s.build_bvh())
+    s = base.copy()
+    s.triangles["v1"][7] = s.triangles["v0"][7]
+    s.triangles["v2"][7] = s.triangles["v0"][7]
+    cases.append(s.build_bvh())
+    for s in cases:
+        nodes, bad = pt.layout_check(s)
+        assert nodes > 0 and bad == 0, (nodes, bad)
+
+
 def test_procedural_scene_counts():
     """The 1M-triangle scene: 16 spheres of 2*256*128 = 65,536 triangles, floor and light quads."""
     p = pt.procedural_params()
