@@ -14,14 +14,18 @@ The default run (one GPU) prints one JSON line with the headline number and, bes
   cpu_baseline     the reference's trace_world on all host cores (about 10 s of host work);
   cpu_baseline_bvh_node   its pre-CUDA bvh_node::hit path on a random sample
   c3               the traversal microbenchmark (9,437,184 triangles, 2^25 rays) in closest-hit and
-                   any-hit modes, with parity on random subsets
+                   any-hit modes, with parity on random subsets and the reference's own query kernel
+                   on the same rays
   render_c2        the progressive renderer on config 2 against the reference's CUDA renderer
                    (bounce limit 8) on the same GPU, images compared bitwise
+  render_c2_depth50   the same at the reference's own bounce limit 50, against its unpatched build
+  render_c1        the Cornell box (config 1) against the reference's CUDA renderer
   cache_c5         the radiance-cache renderer against plain path tracing at 1920x1080: time to
                    the plain method's 1024-spp relMSE and to relMSE <= 1e-3, wall and device time
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--quick]
   python bench.py --workload batch48|cache|mlp|render|c3     one sub-workload as its own line
+  python bench.py --workload render --render-scene cornell    the config-1 render alone
 
 --impl reference times the reference's own CPU traversal (trace_world on host_view, built from
 its sources into oracle/_ref/) on all host threads over a seeded random sample of the same rays.
